@@ -1,0 +1,378 @@
+"""Benchmark of the SmallStrainFFT solve on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload plain128]
+
+One "step" is one complete RVE solve of the workload (every load increment, Newton
+iterations and device MINRES), with the microstructure already resident in HBM.
+Multi-GPU runs are independent replicas (one RVE solve stream per GPU; the path has no
+exchange step), so ``scaling`` is "weak".
+
+Prints one JSON line (rank 0).
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "served RVE solves/s + p50/p99 latency vs plain GPU solve at <=1e-5 stress err"
+
+WORKLOADS = {
+    # Plain method on GPU at scale: cubic elastic 250/150/120, 128^3, 500 periodic
+    # Voronoi grains with uniform SO(3) orientations, uniaxial x strain rate 1e-3 for
+    # 20 steps, float fields/FFT with double residuals and norms, tolerance 1e-6.
+    "plain128": dict(n=128, grains=500, steps=20, dt=1.0, rate=1e-3, gtol=1e-6,
+                     ltol=1e-5, precision="mixed", seed=0),
+    "plain64": dict(n=64, grains=200, steps=20, dt=1.0, rate=1e-3, gtol=1e-6,
+                    ltol=1e-5, precision="mixed", seed=0),
+}
+
+# Algorithmic HBM bytes per voxel of each Krylov-iteration kernel with float fields:
+# planar vectors are 24 B/voxel (6 x 4 B); the half spectrum is 6 x (n/2+1)/n x 8 B.
+def kernel_bytes_per_voxel(n, table_mode=True):
+    spec = 6 * (n // 2 + 1) / n * 8.0
+    kin = 4.0 if table_mode else 84.0
+    return {
+        "zfwd": 24.0 + kin + spec,          # read v, tangent; write spectrum
+        "yfwd": 2 * spec,                    # read + write spectrum
+        "xpass": 2 * spec,
+        "yinv": 2 * spec,
+        "zinv": spec + 3 * 24.0,            # read spectrum, r1, r2; write y
+        "upd1": 3 * 24.0,                   # read y, r2; write y
+        "upd2": 6 * 24.0,                   # read v, w1, w2, x; write w, x
+    }
+
+
+KERNEL_NAMES = ["zfwd", "yfwd", "xpass", "yinv", "zinv", "upd1", "upd2"]
+
+
+def cubic_mandel(C11, C12, C44):
+    s = np.array([1, 1, 1, np.sqrt(2), np.sqrt(2), np.sqrt(2)])
+    V = np.zeros((6, 6))
+    V[:3, :3] = C12
+    V[[0, 1, 2], [0, 1, 2]] = C11
+    V[[3, 4, 5], [3, 4, 5]] = C44
+    return V * np.outer(s, s)
+
+
+def build_microstructure(w):
+    from materialite_b200.microstructure import periodic_voronoi, quaternion_random_rotations
+    n = w["n"]
+    rng = np.random.default_rng(w["seed"])
+    ids = periodic_voronoi((n, n, n), w["grains"], rng)
+    rot = quaternion_random_rotations(w["grains"], rng)
+    return rot, ids.astype(np.int32)
+
+
+def uniaxial_x(rate):
+    mask = np.array([0, 1, 1, 1, 1, 1], dtype=float)
+    er = np.array([rate, 0, 0, 0, 0, 0], dtype=float)
+    zero = np.zeros(6)
+    return mask, (lambda t, dt: er * dt), (lambda t, dt: zero), (lambda t, dt: zero)
+
+
+def read_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.isfile(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for k, name in enumerate(names):
+                    if r[5 + k].strip().lower().startswith("active"):
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world, local):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world, local):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def make_handle(w, rot, ids, device):
+    from materialite_b200.engine import PhaseSpec, SolverHandle
+    mask, *_ = uniaxial_x(w["rate"])
+    n = w["n"]
+    h = SolverHandle((n, n, n), mask, w["precision"], global_tolerance=w["gtol"],
+                     linear_solver_tolerance=w["ltol"], device=device)
+    h.set_phases([PhaseSpec("elastic", cubic_mandel(250.0, 150.0, 120.0))])
+    h.set_microstructure(rot, ids)
+    return h
+
+
+def run_solve(h, w, stats=None):
+    from materialite_b200.engine import solve
+    _, de, ds, s = uniaxial_x(w["rate"])
+    return solve(h, de, ds, s, end_time=w["steps"] * w["dt"], initial_time_increment=w["dt"],
+                 stats=stats)
+
+
+def cpu_sample(w, max_seconds=40.0):
+    """Time the numpy oracle (single process) on the first load increment of the
+    workload, plus its one-off Gamma-hat build, and extrapolate to a full solve."""
+    from oracle import ssfft_oracle as O
+    from materialite_b200.engine import unique_rotations  # noqa: F401
+    rot, ids = build_microstructure(w)
+    n = w["n"]
+    R = rot[ids]
+    mask, de, ds, s = uniaxial_x(w["rate"])
+    t0 = time.perf_counter()
+    G = O.projection_operator((n, n, n), mask)
+    t_build = time.perf_counter() - t0
+    del G
+    load = O.LoadOracle(de, ds, s, mask)
+    t0 = time.perf_counter()
+    O.solve((n, n, n), R, O.ElasticOracle(cubic_mandel(250.0, 150.0, 120.0)), load,
+            end_time=w["dt"], initial_time_increment=w["dt"], global_tolerance=w["gtol"],
+            linear_solver_tolerance=w["ltol"])
+    t_first = time.perf_counter() - t0 - t_build  # solve() rebuilds Gamma-hat once
+    per_solve = t_build + w["steps"] * t_first
+    return per_solve, t_build, t_first
+
+
+def reference_arm(args, w):
+    """--impl reference: the oracle restatement of the reference's numpy path on the host
+    cores.  Each step runs one bounded sample (Gamma-hat build + first load increment)
+    per worker process, all workers in parallel; value = workers / extrapolated solve
+    time."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        mem_workers = max(1, int(psutil.virtual_memory().available / (12 * 2**30)))
+    except Exception:
+        mem_workers = 4
+    workers = max(1, min(cores, mem_workers, 16))
+    ctx = mp.get_context("spawn")
+    times = []
+    with ctx.Pool(workers) as pool:
+        for i in range(args.warmup + args.steps):
+            res = pool.map(_ref_worker, [w] * workers)
+            if i >= args.warmup:
+                times.append(max(r[0] for r in res))
+    per_solve = statistics.mean(times)
+    value = workers / per_solve
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_solve * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded periodic Voronoi, uniform SO(3))",
+            "impl": "reference",
+            "config": {"workload": args.workload, **{k: w[k] for k in ("n", "grains", "steps")},
+                       "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers,
+                             "kind": "port",
+                             "sample": "per worker: Gamma-hat build + first load increment, "
+                                       "extrapolated to all load increments"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _ref_worker(w):
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    return cpu_sample(w)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="plain128", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        reference_arm(args, w)
+        return
+    world, rank, local = dist_setup(args.gpus)
+    from materialite_b200.engine import SolveStats
+    rot, ids = build_microstructure(w)
+    h = make_handle(w, rot, ids, local)
+    for _ in range(args.warmup):
+        run_solve(h, w)
+    _, launches0 = h.stats()
+    barrier(world)
+    sampler = ClockSampler(local)
+    sampler.start()
+    st = SolveStats()
+    h.timer_start()
+    for _ in range(args.steps):
+        run_solve(h, w, st)
+    t = h.timer_stop()
+    clocks = sampler.stop()
+    _, launches1 = h.stats()
+    t_max = max_over_ranks(t, world, local)
+    total_solves = sum_over_ranks(args.steps, world, local)
+    value = total_solves / t_max
+    # accuracy self-check of the timed solve is covered by the parity tests; record the
+    # solver work for context
+    krylov_per_solve = sum(st.krylov_iterations) / args.steps
+    newton_per_solve = sum(st.newton_iterations) / args.steps
+
+    # roofline of the dominant Krylov kernel, timed live with CUDA events on the
+    # handle's stream
+    prof = h.profile_krylov(reps=20)
+    n = w["n"]
+    V = n ** 3
+    bpv = kernel_bytes_per_voxel(n)
+    per_kernel = {k: prof[i] for i, k in enumerate(KERNEL_NAMES)}
+    dom = max(per_kernel, key=per_kernel.get)
+    peak, peak_kind = read_peaks()
+    achieved = bpv[dom] * V / per_kernel[dom] / 1e9
+    iter_bytes = sum(bpv.values()) * V
+    iter_gbs = iter_bytes / prof[7] / 1e9
+
+    # end to end through the host API: upload the microstructure, solve, read back
+    # stress and strain
+    e2e_times = []
+    from materialite_b200.engine import SolverHandle  # noqa: F401
+    h.close()
+    for _ in range(args.e2e_steps):
+        t0 = time.perf_counter()
+        he = make_handle(w, rot, ids, local)
+        out, _ = run_solve(he, w)
+        he.close()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_max = max_over_ranks(statistics.mean(e2e_times), world, local)
+    e2e_value = sum_over_ranks(1.0, world, local) / e2e_max
+    h2d = ids.nbytes + rot.nbytes
+    d2h = 2 * V * 6 * 8
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        per_solve, t_build, t_first = cpu_sample(w)
+        cpu = {"value": 1.0 / per_solve, "unit": "solves/s", "cores": 1, "kind": "port",
+               "sample": f"numpy oracle: Gamma-hat build ({t_build:.1f} s) + first load "
+                         f"increment ({t_first:.1f} s) of this workload, extrapolated to "
+                         f"{w['steps']} increments"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded periodic Voronoi, uniform SO(3) quaternions)",
+            "config": {"workload": f"{args.workload}: plain SmallStrainFFT solve, cubic elastic "
+                                   f"250/150/120, {n}^3, {w['grains']} periodic Voronoi grains, "
+                                   f"uniaxial x 1e-3, {w['steps']} steps, float fields/FFT with "
+                                   f"double residuals and norms, tolerance {w['gtol']}",
+                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2",
+                       "krylov_iterations_per_solve": krylov_per_solve,
+                       "newton_iterations_per_solve": newton_per_solve},
+            "clocks": clocks,
+            "gpu_launches": int(launches1 - launches0),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "peak_kind": peak_kind,
+                         "per_kernel_us": {k: v * 1e6 for k, v in per_kernel.items()},
+                         "krylov_iteration_us": prof[7] * 1e6,
+                         "krylov_iteration_gbs": iter_gbs},
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,275 @@
+// Elementwise and reduction kernels around the Newton loop of SmallStrainFFT.run
+// (small_strain_fft.py:106-246): strain guess, strain update, convergence norms,
+// mean tangent, commit, and layout conversion for read-back.
+#pragma once
+
+#include "common.cuh"
+#include "constitutive.cuh"
+
+// Tangent lookup: table mode (per (orientation, phase) pair) or voxel mode (21 planes).
+template <typename T> struct TangentRef {
+  const T *ktab;
+  const int32_t *gid;
+  const T *kvox;
+  long long V;
+  __device__ __forceinline__ void apply(long long v, const double *x, double *y) const {
+    if (kvox) {
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) acc += (double)kvox[sym_idx(i, j) * V + v] * x[j];
+        y[i] = acc;
+      }
+    } else {
+      const T *k = ktab + (long long)gid[v] * 21;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) acc += (double)k[sym_idx(i, j)] * x[j];
+        y[i] = acc;
+      }
+    }
+  }
+  __device__ __forceinline__ double entry(long long v, int k) const {
+    return kvox ? (double)kvox[k * V + v] : (double)ktab[(long long)gid[v] * 21 + k];
+  }
+};
+
+struct StepVec {
+  double corr[6];  // tangent.mean().inv @ stress_increment, or zero
+  double dEbar[6]; // strain increment alone (first-step stress guess)
+  double dS[6];    // stress increment
+};
+
+// strain = old_strain + dE + old_fluct ; guess = first ? dS + K dEbar : old_stress + dS
+// (small_strain_fft.py:113-123)
+template <typename T>
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    strain_guess_kernel(long long V, StepVec sv, int first_step, int reset_fluct,
+                        const T *__restrict__ eps_old, T *__restrict__ dfl,
+                        const T *__restrict__ sig_old, T *__restrict__ eps,
+                        T *__restrict__ guess, TangentRef<T> K) {
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < V;
+       v += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      T f = dfl[c * V + v];
+      if (reset_fluct) {
+        f = 0;
+        dfl[c * V + v] = 0;
+      }
+      // same association as the reference: (old + dEbar + fluct) + correction
+      double e = (double)eps_old[c * V + v] + sv.dEbar[c];
+      eps[c * V + v] = (T)((e + (double)f) + sv.corr[c]);
+    }
+    if (first_step) {
+      double y[6];
+      K.apply(v, sv.dEbar, y);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) guess[c * V + v] = (T)(sv.dS[c] + y[c]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) guess[c * V + v] = (T)((double)sig_old[c * V + v] + sv.dS[c]);
+    }
+  }
+}
+
+// strain += dx ; old_fluct += dx  (small_strain_fft.py:154-155)
+template <typename T>
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    update_strain_kernel(long long n, const T *__restrict__ dx, T *__restrict__ eps,
+                         T *__restrict__ dfl) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const T d = dx[i];
+    eps[i] += d;
+    dfl[i] += d;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    scale_kernel(long long n, T *__restrict__ x, double f) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] = (T)((double)x[i] * f);
+}
+
+__device__ __forceinline__ double dev_norm6(const double *s) {
+  const double tr3 = (s[0] + s[1] + s[2]) / 3.0;
+  const double a = s[0] - tr3, b = s[1] - tr3, c = s[2] - tr3;
+  return sqrt(a * a + b * b + c * c + s[3] * s[3] + s[4] * s[4] + s[5] * s[5]);
+}
+
+// Convergence quantities of small_strain_fft.py:172-189 in one pass:
+//   out[0..5]  sum of stress      out[6..11] sum of strain
+//   out[12]    max |dev(stress - old_stress)|   out[13] max |K : dx|  (if dx given)
+#define NORM_VALS 14
+template <typename T>
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    newton_norms_kernel(long long V, const T *__restrict__ sig, const T *__restrict__ sig_old,
+                        const T *__restrict__ eps, const T *__restrict__ dx, TangentRef<T> K,
+                        double *partials, unsigned int *ticket, double *out) {
+  __shared__ double red[32];
+  double acc[NORM_VALS];
+#pragma unroll
+  for (int k = 0; k < NORM_VALS; ++k) acc[k] = 0.0;
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < V;
+       v += (long long)gridDim.x * blockDim.x) {
+    double s[6], d[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      s[c] = (double)sig[c * V + v];
+      acc[c] += s[c];
+      acc[6 + c] += (double)eps[c * V + v];
+      d[c] = s[c] - (double)sig_old[c * V + v];
+    }
+    acc[12] = fmax(acc[12], dev_norm6(d));
+    if (dx) {
+      double x[6], y[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) x[c] = (double)dx[c * V + v];
+      K.apply(v, x, y);
+      double n2 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) n2 += y[c] * y[c];
+      acc[13] = fmax(acc[13], sqrt(n2));
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NORM_VALS; ++k) {
+    const double r = (k < 12) ? block_sum(acc[k], red) : block_max(acc[k], red);
+    if (threadIdx.x == 0) partials[(size_t)blockIdx.x * NORM_VALS + k] = r;
+  }
+  if (!last_block_arrives(ticket)) return;
+  for (int k = 0; k < NORM_VALS; ++k) {
+    const double r = (k < 12) ? ordered_sum(partials + k, gridDim.x, NORM_VALS, red)
+                              : ordered_max(partials + k, gridDim.x, NORM_VALS, red);
+    if (threadIdx.x == 0) out[k] = r;
+  }
+  if (threadIdx.x == 0) *ticket = 0;
+}
+
+// Sum of the tangent over all points (21 packed entries) for tangent.mean().inv
+// (small_strain_fft.py:119-120).
+template <typename T>
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    tangent_sum_kernel(long long V, TangentRef<T> K, double *partials, unsigned int *ticket,
+                       double *out) {
+  __shared__ double red[32];
+  double acc[21];
+#pragma unroll
+  for (int k = 0; k < 21; ++k) acc[k] = 0.0;
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < V;
+       v += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < 21; ++k) acc[k] += K.entry(v, k);
+  }
+#pragma unroll
+  for (int k = 0; k < 21; ++k) {
+    const double r = block_sum(acc[k], red);
+    if (threadIdx.x == 0) partials[(size_t)blockIdx.x * 21 + k] = r;
+  }
+  if (!last_block_arrives(ticket)) return;
+  for (int k = 0; k < 21; ++k) {
+    const double r = ordered_sum(partials + k, gridDim.x, 21, red);
+    if (threadIdx.x == 0) out[k] = r;
+  }
+  if (threadIdx.x == 0) *ticket = 0;
+}
+
+// Planar T (width planes of V) -> point-major float64 (V x width).
+template <typename T>
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    to_point_major_kernel(long long V, int width, const T *__restrict__ src,
+                          double *__restrict__ dst) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < V * width;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long v = i / width;
+    const int c = (int)(i - v * width);
+    dst[i] = (double)src[c * V + v];
+  }
+}
+
+// Point-major float64 (V x 6) -> planar T.
+template <typename T>
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    from_point_major_kernel(long long V, const double *__restrict__ src, T *__restrict__ dst) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < V * 6;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long v = i / 6;
+    const int c = (int)(i - v * 6);
+    dst[c * V + v] = (T)src[i];
+  }
+}
+
+// Committed crystal-frame plastic strains -> specimen frame, point-major
+// (elastic_viscoplastic.py:258-263).
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    plastic_to_specimen_kernel(long long V, const double *__restrict__ ep,
+                               const int32_t *__restrict__ orient,
+                               const double *__restrict__ rm_tab, double *__restrict__ dst) {
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < V;
+       v += (long long)gridDim.x * blockDim.x) {
+    const double *Rm = rm_tab + (long long)orient[v] * 36;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      double acc = 0.0;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) acc += Rm[j * 6 + i] * ep[j * V + v];
+      dst[v * 6 + i] = acc;
+    }
+  }
+}
+
+// Initial EVP state: slip resistances g0 on EVP voxels, zero elsewhere.
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    evp_init_kernel(long long V, int nslip_max, const int32_t *__restrict__ phase,
+                    const PhaseParams *__restrict__ params, double *g_a, double *g_b,
+                    double *g_old) {
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < V;
+       v += (long long)gridDim.x * blockDim.x) {
+    const PhaseParams &P = params[phase ? phase[v] : 0];
+    for (int al = 0; al < nslip_max; ++al) {
+      const double g = (P.kind == PHASE_EVP && al < P.nslip) ? P.g0 : 0.0;
+      g_a[al * V + v] = g;
+      g_b[al * V + v] = g;
+      g_old[al * V + v] = g;
+    }
+  }
+}
+
+// Voxel-mode tangent initialisation: K = Rm^T C Rm for every voxel of every phase
+// (elastic.py:23-27, elastic_viscoplastic.py:89).
+template <typename T>
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    init_kvox_kernel(long long V, const int32_t *__restrict__ phase,
+                     const int32_t *__restrict__ orient, const PhaseParams *__restrict__ params,
+                     const double *__restrict__ rm_tab, T *__restrict__ kvox) {
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < V;
+       v += (long long)gridDim.x * blockDim.x) {
+    const PhaseParams &P = params[phase ? phase[v] : 0];
+    const double *Rm = rm_tab + (long long)orient[v] * 36;
+    double CR[36];
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int b = 0; b < 6; ++b) {
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) acc += P.C[i * 6 + j] * Rm[j * 6 + b];
+        CR[i * 6 + b] = acc;
+      }
+#pragma unroll
+    for (int a = 0; a < 6; ++a)
+#pragma unroll
+      for (int b = a; b < 6; ++b) {
+        double acc = 0.0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) acc += Rm[i * 6 + a] * CR[i * 6 + b];
+        kvox[sym_idx(a, b) * V + v] = (T)acc;
+      }
+  }
+}

@@ -1,0 +1,1213 @@
+// libssfft: C ABI and host driver of the sm_100a SmallStrainFFT solver.
+//
+// The Newton / Krylov structure follows materialite's SmallStrainFFT.run
+// (materialite/models/small_strain_fft/small_strain_fft.py:106-246): one call to
+// ssfft_step is one load increment (strain guess, Newton loop, MINRES per Newton
+// iteration, convergence tests); the time loop, adaptive dt and output collection stay
+// with the caller, as in the reference.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ssfft.h"
+#include "common.cuh"
+#include "constitutive.cuh"
+#include "fft.cuh"
+#include "fields.cuh"
+#include "krylov.cuh"
+#include "projector.cuh"
+
+// ---------------------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(SSFFT_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+#define CKR(expr)          \
+  do {                     \
+    int r_ = (expr);       \
+    if (r_ != 0) return r_; \
+  } while (0)
+
+extern "C" const char *ssfft_last_error(void) { return g_last_error.c_str(); }
+
+// ---------------------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------------------
+enum { TK_INIT = 0, TK_ZINV, TK_UPD1, TK_UPD2, TK_NORMS, TK_TSUM, TK_COUNT };
+#define MAX_PARTIAL_BLOCKS 65536
+
+struct ssfft_handle {
+  ssfft_config cfg;
+  bool fp64;
+  size_t rs;  // sizeof(real)
+  cudaStream_t stream;
+  int nx, ny, nz, hz;
+  long long V, S;
+  AxisPlan px, py, pz;
+  int lz, ky, kx;
+  size_t smem_z, smem_y, smem_x;
+  int red_blocks;  // grid of grid-stride reduction kernels
+  void *tw[2][3], *tn[2][3];  // [0]: float, [1]: double tables per axis
+  // fields (planar, real type)
+  void *eps, *sig, *sig_old, *eps_old, *dfl, *guess, *b;
+  void *kr[6];
+  void *spec;
+  // microstructure
+  bool micro_set;
+  bool voxel_mode;
+  int n_orient, n_gid;
+  int32_t *orient, *phase, *gid;
+  double *rm_tab;
+  void *ktab, *kvox, *kvox_old;
+  PhaseParams hparams[SSFFT_MAX_PHASES];
+  bool phase_set[SSFFT_MAX_PHASES];
+  PhaseParams *dparams;
+  bool any_evp;
+  int nslip_max;
+  // EVP state
+  double *g_buf[2];
+  int g_cur;
+  double *g_old, *ep_old, *ep_trial, *Gam_old, *Gam_trial, *gam_old, *gam_trial;
+  // reductions / scalars
+  double *partials;
+  unsigned int *tickets;
+  double *results;   // [0..13] norms, [16..36] tangent sum, [40] max|b|
+  MinresState *st;
+  int *citers, *cfail;
+  double *h_results;  // pinned mirror
+  MinresState *h_st;
+  int *h_cint;
+  cudaEvent_t ev0, ev1, tev0, tev1;
+  cudaEvent_t pev[9];
+  double last_step_seconds;
+  long long launches;
+};
+
+// ---------------------------------------------------------------------------------------
+// planning
+// ---------------------------------------------------------------------------------------
+static bool make_plan(int n, AxisPlan &p) {
+  p.n = n;
+  p.nrad = 0;
+  int m = n;
+  auto push = [&](int r) {
+    if (p.nrad >= SSFFT_MAX_STAGES) return false;
+    p.rad[p.nrad++] = r;
+    m /= r;
+    return true;
+  };
+  while (m % 8 == 0)
+    if (!push(8)) return false;
+  while (m % 4 == 0)
+    if (!push(4)) return false;
+  while (m % 2 == 0)
+    if (!push(2)) return false;
+  for (int f = 3; m > 1; f += 2) {
+    while (m % f == 0) {
+      if (f > SSFFT_MAX_GENERIC_RADIX) return false;
+      if (!push(f)) return false;
+    }
+  }
+  return true;
+}
+
+template <typename T> static std::vector<T> twiddles(int n) {
+  std::vector<T> tw(2 * (size_t)n);
+  for (int k = 0; k < n; ++k) {
+    const long double a = -2.0L * 3.14159265358979323846264338327950288L * k / n;
+    tw[2 * k] = (T)std::cos(a);
+    tw[2 * k + 1] = (T)std::sin(a);
+  }
+  return tw;
+}
+
+// tan(pi f) for numpy's fftfreq ordering (first `count` entries).
+template <typename T> static std::vector<T> tan_table(int n, int count) {
+  std::vector<T> t(count);
+  for (int k = 0; k < count; ++k) {
+    const int kk = (k < (n + 1) / 2) ? k : k - n;  // fftfreq index
+    const long double f = (long double)kk / n;
+    if (2 * kk == -n || 2 * kk == n)
+      t[k] = (T)0;  // Nyquist plane: operator is zeroed there
+    else
+      t[k] = (T)std::tan(3.14159265358979323846264338327950288L * f);
+  }
+  return t;
+}
+
+template <typename T> static Grid<T> make_grid(const ssfft_handle *h) {
+  Grid<T> g;
+  g.nx = h->nx;
+  g.ny = h->ny;
+  g.nz = h->nz;
+  g.hz = h->hz;
+  g.V = h->V;
+  g.S = h->S;
+  g.px = h->px;
+  g.py = h->py;
+  g.pz = h->pz;
+  const int p = sizeof(T) == 8 ? 1 : 0;
+  g.twx = (const cplx<T> *)h->tw[p][0];
+  g.twy = (const cplx<T> *)h->tw[p][1];
+  g.twz = (const cplx<T> *)h->tw[p][2];
+  g.tanx = (const T *)h->tn[p][0];
+  g.tany = (const T *)h->tn[p][1];
+  g.tanz = (const T *)h->tn[p][2];
+  g.scale = (T)(1.0 / (double)h->V);
+  for (int c = 0; c < 6; ++c) g.mask[c] = (T)((h->cfg.stress_mask[c] != 0.0) ? 1.0 : 0.0);
+  g.lz = h->lz;
+  g.ky = h->ky;
+  g.kx = h->kx;
+  return g;
+}
+
+static int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+static size_t field_bytes(const ssfft_handle *h, int planes) {
+  return (size_t)planes * (size_t)h->V * h->rs;
+}
+
+template <typename F> static int smem_attr(F f, int m) {
+  CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, m));
+  return 0;
+}
+
+// Opt every shared-memory-hungry kernel instantiation into up to `smax` bytes.
+template <typename T, typename TF> static int set_kernel_attrs(size_t smax) {
+  const int m = (int)smax;
+  CKR(smem_attr(zfwd_kernel<T, TF, PRO_INPUT>, m));
+  CKR(smem_attr(zfwd_kernel<T, TF, PRO_RESIDUAL>, m));
+  CKR(smem_attr(ypass_kernel<T, false>, m));
+  CKR(smem_attr(ypass_kernel<T, true>, m));
+  CKR(smem_attr(xpass_kernel<T>, m));
+  CKR(smem_attr(zinv_kernel<T, TF, EPI_STORE>, m));
+  CKR(smem_attr(zinv_kernel<T, TF, EPI_RESIDUAL>, m));
+  if (sizeof(T) == sizeof(TF)) {
+    CKR(smem_attr(zfwd_kernel<T, T, PRO_TANGENT_TABLE>, m));
+    CKR(smem_attr(zfwd_kernel<T, T, PRO_TANGENT_VOXEL>, m));
+    CKR(smem_attr(zinv_kernel<T, T, EPI_MINRES>, m));
+  }
+  return 0;
+}
+
+static const size_t SMEM_LIMIT = 200 * 1024;
+
+static int plan_tiles(ssfft_handle *h) {
+  // tiles are sized for double-precision transforms, which both modes run (the mixed mode
+  // computes its equilibrium residual in double)
+  const size_t cs = 16;  // complex bytes
+  // z passes: 3 paired lines per (x,y) line, two buffers, twiddles
+  h->lz = std::max(1, std::min(32, 2048 / (3 * h->nz)));
+  h->lz = (int)std::min<long long>(h->lz, (long long)h->nx * h->ny);
+  h->smem_z = (2 * 3 * (size_t)h->lz * h->nz + h->nz) * cs;
+  // y pass: ky kz-columns
+  h->ky = std::min(h->hz, 16);
+  while (h->ky > 1 && (2 * (size_t)h->ky * h->ny + h->ny) * cs > 96 * 1024) h->ky /= 2;
+  h->smem_y = (2 * (size_t)h->ky * h->ny + h->ny) * cs;
+  // x pass: 6 components of kx kz-columns
+  h->kx = std::min(h->hz, 8);
+  while (h->kx > 1 && (12 * (size_t)h->kx * h->nx + h->nx) * cs > 100 * 1024) h->kx /= 2;
+  h->smem_x = (12 * (size_t)h->kx * h->nx + h->nx) * cs;
+  if (h->smem_z > SMEM_LIMIT || h->smem_y > SMEM_LIMIT || h->smem_x > SMEM_LIMIT)
+    return fail(SSFFT_E_UNSUPPORTED, "grid too large for the shared-memory FFT passes");
+  if (div_up((long long)h->nx * h->ny, h->lz) > MAX_PARTIAL_BLOCKS)
+    return fail(SSFFT_E_UNSUPPORTED, "grid too large for the reduction partials");
+  return 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// projector launches
+// ---------------------------------------------------------------------------------------
+template <typename T, typename TF, int PRO, int EPI>
+static int launch_projector(ssfft_handle *h, const ProArgs<TF> &pa, const EpiArgs<TF> &ea,
+                            const MinresState *st) {
+  Grid<T> g = make_grid<T>(h);
+  cplx<T> *spec = (cplx<T> *)h->spec;
+  const size_t cs = sizeof(cplx<T>);
+  const size_t sz = (6 * (size_t)h->lz * h->nz + h->nz) * cs;
+  const size_t sy = (2 * (size_t)h->ky * h->ny + h->ny) * cs;
+  const size_t sx = (12 * (size_t)h->kx * h->nx + h->nx) * cs;
+  const int nzb = div_up((long long)h->nx * h->ny, h->lz);
+  zfwd_kernel<T, TF, PRO><<<nzb, SSFFT_THREADS, sz, h->stream>>>(g, pa, spec);
+  ypass_kernel<T, false><<<dim3(div_up(h->hz, h->ky), h->nx, 6), SSFFT_THREADS, sy,
+                           h->stream>>>(g, spec, st);
+  xpass_kernel<T><<<dim3(div_up(h->hz, h->kx), h->ny), SSFFT_THREADS, sx, h->stream>>>(
+      g, spec, st);
+  ypass_kernel<T, true><<<dim3(div_up(h->hz, h->ky), h->nx, 6), SSFFT_THREADS, sy,
+                          h->stream>>>(g, spec, st);
+  zinv_kernel<T, TF, EPI><<<nzb, SSFFT_THREADS, sz, h->stream>>>(g, ea, spec);
+  h->launches += 5;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+template <typename T> static TangentRef<T> tangent_ref(const ssfft_handle *h) {
+  TangentRef<T> K;
+  K.ktab = (const T *)h->ktab;
+  K.gid = h->gid;
+  K.kvox = h->voxel_mode ? (const T *)h->kvox : nullptr;
+  K.V = h->V;
+  return K;
+}
+
+// b = P(Sbar - sigma) into h->b, max|b| into results[40].  The transform always runs in
+// double: in the mixed mode the float stress field is read and b is stored as float, but
+// the equilibrium residual and its norm are double-precision quantities.
+template <typename T> static int residual(ssfft_handle *h, const double sbar[6]) {
+  ProArgs<T> pa{};
+  pa.in = (const T *)h->sig;
+  for (int c = 0; c < 6; ++c) pa.sbar[c] = sbar[c];
+  EpiArgs<T> ea{};
+  ea.out = (T *)h->b;
+  ea.partials = h->partials;
+  ea.ticket = h->tickets + TK_ZINV;
+  ea.result = h->results + 40;
+  return launch_projector<double, T, PRO_RESIDUAL, EPI_RESIDUAL>(h, pa, ea, nullptr);
+}
+
+// Mixed mode only: project a Newton correction back onto compatible strain fields with a
+// double-precision transform (x <- Gamma-hat : x, an identity in exact arithmetic).  Float
+// Krylov iterates pick up round-off in the null space of Gamma-hat K, which the
+// equilibrium test cannot see; this removes it.
+template <typename T> static int reproject(ssfft_handle *h, T *x) {
+  ProArgs<T> pa{};
+  pa.in = x;
+  EpiArgs<T> ea{};
+  ea.out = x;
+  return launch_projector<double, T, PRO_INPUT, EPI_STORE>(h, pa, ea, nullptr);
+}
+
+// ---------------------------------------------------------------------------------------
+// MINRES driver
+// ---------------------------------------------------------------------------------------
+#define KRYLOV_CHUNK 8
+#define MIXED_RTOL_FLOOR 1.0e-6
+
+template <typename T> static int run_minres(ssfft_handle *h, long long *iters, T **xout) {
+  const long long n = 6 * h->V;
+  T *R1 = (T *)h->kr[0], *R2 = (T *)h->kr[1], *W = (T *)h->kr[2], *W1 = (T *)h->kr[3],
+    *W2 = (T *)h->kr[4], *X = (T *)h->kr[5];
+  const long long maxiter =
+      h->cfg.max_krylov_iterations > 0 ? h->cfg.max_krylov_iterations : 5 * n;
+  // float Krylov vectors cannot resolve relative residuals much below 1e-6
+  const double rtol = h->fp64 ? h->cfg.linear_solver_tolerance
+                              : std::max(h->cfg.linear_solver_tolerance, MIXED_RTOL_FLOOR);
+  minres_init_kernel<T><<<h->red_blocks, SSFFT_THREADS, 0, h->stream>>>(
+      (const T *)h->b, R1, R2, X, W, W2, n, h->st, rtol, maxiter,
+      h->partials, h->tickets + TK_INIT);
+  h->launches += 1;
+  CK(cudaGetLastError());
+  const bool vox = h->voxel_mode;
+  for (;;) {
+    for (int i = 0; i < KRYLOV_CHUNK; ++i) {
+      ProArgs<T> pa{};
+      pa.in = R2;
+      pa.gid = h->gid;
+      pa.ktab = (const T *)h->ktab;
+      pa.kvox = (const T *)h->kvox;
+      pa.st = h->st;
+      EpiArgs<T> ea{};
+      ea.out = R1;
+      ea.r2 = R2;
+      ea.st = h->st;
+      ea.partials = h->partials;
+      ea.ticket = h->tickets + TK_ZINV;
+      if (vox)
+        CKR((launch_projector<T, T, PRO_TANGENT_VOXEL, EPI_MINRES>(h, pa, ea, h->st)));
+      else
+        CKR((launch_projector<T, T, PRO_TANGENT_TABLE, EPI_MINRES>(h, pa, ea, h->st)));
+      minres_upd1_kernel<T><<<h->red_blocks, SSFFT_THREADS, 0, h->stream>>>(
+          R1, R2, n, h->st, h->partials, h->tickets + TK_UPD1);
+      std::swap(R1, R2);
+      minres_upd2_kernel<T><<<h->red_blocks, SSFFT_THREADS, 0, h->stream>>>(
+          R1, W2, W, W1, X, n, h->st, h->partials, h->tickets + TK_UPD2);
+      T *old_w1 = W1;
+      W1 = W2;
+      W2 = W;
+      W = old_w1;
+      h->launches += 2;
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->h_st, h->st, sizeof(MinresState), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->h_st->done) break;
+  }
+  if (h->h_st->istop == 9) return fail(SSFFT_E_NAN, "non-finite value in the Krylov solve");
+  *iters = h->h_st->itn;
+  *xout = X;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// constitutive call
+// ---------------------------------------------------------------------------------------
+template <typename T>
+static int constitutive(ssfft_handle *h, double dt, int *iters, int *failed) {
+  CK(cudaMemsetAsync(h->citers, 0, 2 * sizeof(int), h->stream));
+  ConstArgs<T> a{};
+  a.V = h->V;
+  a.eps = (const T *)h->eps;
+  a.guess = (const T *)h->guess;
+  a.sig = (T *)h->sig;
+  a.kvox = h->voxel_mode ? (T *)h->kvox : nullptr;
+  a.ktab = (const T *)h->ktab;
+  a.gid = h->gid;
+  a.phase = h->phase;
+  a.orient = h->orient;
+  a.params = h->dparams;
+  a.rm_tab = h->rm_tab;
+  if (h->any_evp) {
+    a.g_in = h->g_buf[h->g_cur];
+    a.g_out = h->g_buf[1 - h->g_cur];
+    a.g_old = h->g_old;
+    a.ep_old = h->ep_old;
+    a.ep_trial = h->ep_trial;
+    a.Gam_old = h->Gam_old;
+    a.Gam_trial = h->Gam_trial;
+    a.gam_old = h->gam_old;
+    a.gam_trial = h->gam_trial;
+  }
+  a.dt = dt;
+  a.max_iters = h->citers;
+  a.failed = h->cfail;
+  const int blocks = std::max(1, std::min(div_up(h->V, 128), 148 * 16));
+  constitutive_kernel<T><<<blocks, 128, 0, h->stream>>>(a);
+  h->launches += 1;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->h_cint, h->citers, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  *iters = h->h_cint[0];
+  *failed = h->h_cint[1];
+  if (!*failed && h->any_evp) h->g_cur = 1 - h->g_cur;
+  return 0;
+}
+
+template <typename T> static int norms(ssfft_handle *h, const T *dx) {
+  newton_norms_kernel<T><<<h->red_blocks, SSFFT_THREADS, 0, h->stream>>>(
+      h->V, (const T *)h->sig, (const T *)h->sig_old, (const T *)h->eps, dx, tangent_ref<T>(h),
+      h->partials, h->tickets + TK_NORMS, h->results);
+  h->launches += 1;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->h_results, h->results, 48 * sizeof(double), cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+static double mean_von_mises(const double *sums, long long V) {
+  double m[6];
+  for (int c = 0; c < 6; ++c) m[c] = sums[c] / (double)V;
+  const double tr3 = (m[0] + m[1] + m[2]) / 3.0;
+  double s = 0.0;
+  for (int c = 0; c < 6; ++c) {
+    const double d = (c < 3) ? m[c] - tr3 : m[c];
+    s += d * d;
+  }
+  return std::sqrt(s) * std::sqrt(1.5);
+}
+
+// 6x6 inverse by Gauss-Jordan with partial pivoting (host, double).
+static bool inv6(const double *A, double *Ainv) {
+  double a[6][12];
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 12; ++j) a[i][j] = (j < 6) ? A[i * 6 + j] : (j - 6 == i ? 1.0 : 0.0);
+  for (int c = 0; c < 6; ++c) {
+    int p = c;
+    for (int r = c + 1; r < 6; ++r)
+      if (std::fabs(a[r][c]) > std::fabs(a[p][c])) p = r;
+    if (a[p][c] == 0.0) return false;
+    if (p != c)
+      for (int j = 0; j < 12; ++j) std::swap(a[p][j], a[c][j]);
+    const double d = a[c][c];
+    for (int j = 0; j < 12; ++j) a[c][j] /= d;
+    for (int r = 0; r < 6; ++r)
+      if (r != c) {
+        const double f = a[r][c];
+        if (f != 0.0)
+          for (int j = 0; j < 12; ++j) a[r][j] -= f * a[c][j];
+      }
+  }
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) Ainv[i * 6 + j] = a[i][j + 6];
+  return true;
+}
+
+template <typename T> static void restore_tangent(ssfft_handle *h) {
+  if (h->voxel_mode)
+    cudaMemcpyAsync(h->kvox, h->kvox_old, field_bytes(h, 21), cudaMemcpyDeviceToDevice,
+                    h->stream);
+}
+
+// One load increment (small_strain_fft.py:106-211).
+template <typename T> static int step_impl(ssfft_handle *h, const ssfft_step_in *in,
+                                           ssfft_step_out *out) {
+  memset(out, 0, sizeof(*out));
+  CK(cudaEventRecord(h->ev0, h->stream));
+  const long long V = h->V;
+  const int eb = std::max(1, std::min(div_up(V, SSFFT_THREADS), 148 * 16));
+  StepVec sv{};
+  for (int c = 0; c < 6; ++c) {
+    sv.dEbar[c] = in->strain_increment[c];
+    sv.dS[c] = in->stress_increment[c];
+    sv.corr[c] = 0.0;
+  }
+  bool all_small = true;
+  for (int c = 0; c < 6; ++c)
+    if (!(in->stress_increment[c] < 1.0e-14)) all_small = false;
+  if (!all_small) {  // strain += tangent.mean().inv @ stress_increment
+    tangent_sum_kernel<T><<<h->red_blocks, SSFFT_THREADS, 0, h->stream>>>(
+        V, tangent_ref<T>(h), h->partials, h->tickets + TK_TSUM, h->results + 16);
+    h->launches += 1;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->h_results, h->results, 48 * sizeof(double), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    double Km[36], Ki[36];
+    for (int i = 0; i < 6; ++i)
+      for (int j = 0; j < 6; ++j) Km[i * 6 + j] = h->h_results[16 + sym_idx(i, j)] / (double)V;
+    if (!inv6(Km, Ki)) return fail(SSFFT_E_INVALID, "mean tangent is singular");
+    for (int i = 0; i < 6; ++i) {
+      double acc = 0.0;
+      for (int j = 0; j < 6; ++j) acc += Ki[i * 6 + j] * in->stress_increment[j];
+      sv.corr[i] = acc;
+    }
+  }
+  strain_guess_kernel<T><<<eb, SSFFT_THREADS, 0, h->stream>>>(
+      V, sv, in->time_step_id == 0, in->reset_fluctuation, (const T *)h->eps_old, (T *)h->dfl,
+      (const T *)h->sig_old, (T *)h->eps, (T *)h->guess, tangent_ref<T>(h));
+  h->launches += 1;
+  CK(cudaGetLastError());
+
+  const double gtol = h->cfg.global_tolerance;
+  const double stol = h->cfg.strain_correction_tolerance;
+  const int max_newton = h->cfg.max_newton_iterations > 0 ? h->cfg.max_newton_iterations : 100;
+  bool converged = false;
+  int it = 0, max_cit = 0;
+  double eq_err = 0.0, mvm = 0.0, s_err = 0.0;
+  long long kits_total = 0;
+  int solves = 0;
+  while (!converged) {
+    ++it;
+    if (it == 1) {
+      int cit, cf;
+      CKR(constitutive<T>(h, in->dt, &cit, &cf));
+      if (cf) {
+        restore_tangent<T>(h);
+        out->constitutive_failed = 1;
+        break;
+      }
+      max_cit = std::max(max_cit, cit);
+      CKR(residual<T>(h, in->mean_applied_stress));
+      CKR(norms<T>(h, nullptr));
+      mvm = mean_von_mises(h->h_results, V);
+      eq_err = h->h_results[40] / mvm;
+      CK(cudaMemcpyAsync(h->guess, h->sig, field_bytes(h, 6), cudaMemcpyDeviceToDevice,
+                         h->stream));
+    }
+    const double old_eq = std::max(eq_err, gtol);
+    long long kits = 0;
+    T *X = nullptr;
+    CKR(run_minres<T>(h, &kits, &X));
+    kits_total += kits;
+    ++solves;
+    if (!h->fp64) CKR(reproject<T>(h, X));
+    update_strain_kernel<T><<<eb, SSFFT_THREADS, 0, h->stream>>>(6 * V, X, (T *)h->eps,
+                                                                  (T *)h->dfl);
+    h->launches += 1;
+    int cit, cf;
+    CKR(constitutive<T>(h, in->dt, &cit, &cf));
+    if (cf) {
+      restore_tangent<T>(h);
+      out->constitutive_failed = 1;
+      break;
+    }
+    max_cit = std::max(max_cit, cit);
+    CKR(residual<T>(h, in->mean_applied_stress));
+    CKR(norms<T>(h, X));
+    mvm = mean_von_mises(h->h_results, V);
+    const double tavg = (in->summed_von_mises_stress + mvm) / (double)(in->time_step_id + 1);
+    if (mvm / tavg < 1.0e-12) mvm = tavg;
+    eq_err = h->h_results[40] / mvm;
+    double max_ds = h->h_results[12] * std::sqrt(1.5);
+    if (max_ds / mvm < 1.0e-12) max_ds = mvm;
+    s_err = h->h_results[13] / max_ds;
+    const double p_err = s_err * eq_err / old_eq;
+    if (eq_err < gtol && (s_err < stol || p_err < stol || in->time_step_id == 0 || eq_err < 1e-8))
+      converged = true;
+    CK(cudaMemcpyAsync(h->guess, h->sig, field_bytes(h, 6), cudaMemcpyDeviceToDevice,
+                       h->stream));
+    if (it == max_newton && !converged) break;
+  }
+  CK(cudaEventRecord(h->ev1, h->stream));
+  CK(cudaEventSynchronize(h->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  h->last_step_seconds = ms * 1e-3;
+  out->converged = converged ? 1 : 0;
+  out->newton_iterations = it;
+  out->max_constitutive_iterations = max_cit;
+  out->krylov_iterations = kits_total;
+  out->linear_solves = solves;
+  out->equilibrium_error = eq_err;
+  out->scaled_strain_error = s_err;
+  out->mean_von_mises_stress = mvm;
+  for (int c = 0; c < 6; ++c) {
+    out->mean_stress[c] = h->h_results[c] / (double)V;
+    out->mean_strain[c] = h->h_results[6 + c] / (double)V;
+  }
+  if (!std::isfinite(eq_err) && converged) out->status = SSFFT_E_NAN;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------
+static void free_handle(ssfft_handle *h) {
+  if (!h) return;
+  for (int p = 0; p < 2; ++p)
+    for (int a = 0; a < 3; ++a) {
+      if (h->tw[p][a]) cudaFree(h->tw[p][a]);
+      if (h->tn[p][a]) cudaFree(h->tn[p][a]);
+    }
+  void *ptrs[] = {h->eps, h->sig,
+                  h->sig_old, h->eps_old, h->dfl, h->guess, h->b, h->kr[0], h->kr[1],
+                  h->kr[2], h->kr[3], h->kr[4], h->kr[5], h->spec, h->orient, h->phase,
+                  h->gid, h->rm_tab, h->ktab, h->kvox, h->kvox_old, h->dparams,
+                  h->g_buf[0], h->g_buf[1], h->g_old, h->ep_old, h->ep_trial, h->Gam_old,
+                  h->Gam_trial, h->gam_old, h->gam_trial, h->partials, h->tickets,
+                  h->results, h->st, h->citers};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (h->h_results) cudaFreeHost(h->h_results);
+  if (h->h_st) cudaFreeHost(h->h_st);
+  if (h->h_cint) cudaFreeHost(h->h_cint);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->tev0) cudaEventDestroy(h->tev0);
+  if (h->tev1) cudaEventDestroy(h->tev1);
+  for (int k = 0; k < 9; ++k)
+    if (h->pev[k]) cudaEventDestroy(h->pev[k]);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+#define ALLOC(ptr, bytes)                                                           \
+  do {                                                                              \
+    cudaError_t e_ = cudaMalloc((void **)&(ptr), (bytes));                          \
+    if (e_ != cudaSuccess) {                                                        \
+      cudaGetLastError();                                                           \
+      return fail(SSFFT_E_NOMEM, std::string("cudaMalloc ") + #ptr + ": " +         \
+                                     cudaGetErrorString(e_));                       \
+    }                                                                               \
+  } while (0)
+
+static int validate_config(const ssfft_config *cfg) {
+  if (!cfg) return fail(SSFFT_E_INVALID, "null config");
+  for (int d = 0; d < 3; ++d)
+    if (cfg->n[d] < 1 || cfg->n[d] > 1024) return fail(SSFFT_E_UNSUPPORTED, "grid size out of range");
+  if (cfg->precision != SSFFT_FP64 && cfg->precision != SSFFT_MIXED)
+    return fail(SSFFT_E_INVALID, "precision must be SSFFT_FP64 or SSFFT_MIXED");
+  for (int c = 0; c < 6; ++c)
+    if (cfg->stress_mask[c] != 0.0 && cfg->stress_mask[c] != 1.0)
+      return fail(SSFFT_E_INVALID, "stress mask can only have zeros and ones");
+  AxisPlan p;
+  for (int d = 0; d < 3; ++d)
+    if (!make_plan(cfg->n[d], p))
+      return fail(SSFFT_E_UNSUPPORTED, "grid size has a prime factor above 32");
+  return 0;
+}
+
+extern "C" int ssfft_estimate_bytes(const ssfft_config *cfg, int any_evp, int n_slip,
+                                    size_t *bytes) {
+  CKR(validate_config(cfg));
+  const size_t V = (size_t)cfg->n[0] * cfg->n[1] * cfg->n[2];
+  const size_t rs = cfg->precision == SSFFT_FP64 ? 8 : 4;
+  const size_t S = (size_t)cfg->n[0] * cfg->n[1] * (cfg->n[2] / 2 + 1);
+  size_t b = 13 * 6 * V * rs + 6 * S * 16 + 3 * V * 4;
+  if (any_evp) b += 2 * 21 * V * rs + (5 * (size_t)n_slip + 12 + 2) * V * 8;
+  b += (size_t)MAX_PARTIAL_BLOCKS * 21 * 8 + (1 << 20);
+  *bytes = b;
+  return 0;
+}
+
+extern "C" int ssfft_create(const ssfft_config *cfg, ssfft_handle **out) {
+  if (!out) return fail(SSFFT_E_INVALID, "null output pointer");
+  *out = nullptr;
+  CKR(validate_config(cfg));
+  CK(cudaSetDevice(cfg->device));
+  ssfft_handle *h = new ssfft_handle();
+  memset((void *)h, 0, sizeof(ssfft_handle));
+  h->cfg = *cfg;
+  h->fp64 = cfg->precision == SSFFT_FP64;
+  h->rs = h->fp64 ? 8 : 4;
+  h->nx = cfg->n[0];
+  h->ny = cfg->n[1];
+  h->nz = cfg->n[2];
+  h->hz = h->nz / 2 + 1;
+  h->V = (long long)h->nx * h->ny * h->nz;
+  h->S = (long long)h->nx * h->ny * h->hz;
+  make_plan(h->nx, h->px);
+  make_plan(h->ny, h->py);
+  make_plan(h->nz, h->pz);
+  int rc = plan_tiles(h);
+  if (rc) {
+    free_handle(h);
+    return rc;
+  }
+  h->red_blocks = std::max(1, std::min(div_up(6 * h->V, SSFFT_THREADS), 148 * 8));
+  auto body = [&]() -> int {
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&h->ev0));
+    CK(cudaEventCreate(&h->ev1));
+    CK(cudaEventCreate(&h->tev0));
+    CK(cudaEventCreate(&h->tev1));
+    for (int k = 0; k < 9; ++k) CK(cudaEventCreate(&h->pev[k]));
+    // FFT tables: float ones for the mixed-mode Krylov transforms, double ones for every
+    // double-precision transform (all transforms of the FP64 mode, residual and
+    // re-projection of the mixed mode)
+    const int dims[3] = {h->nx, h->ny, h->nz};
+    const int tcount[3] = {h->nx, h->ny, h->hz};
+    for (int p = (h->fp64 ? 1 : 0); p < 2; ++p)
+      for (int a = 0; a < 3; ++a) {
+        const size_t es = p ? 8 : 4;
+        ALLOC(h->tw[p][a], (size_t)dims[a] * 2 * es);
+        ALLOC(h->tn[p][a], (size_t)tcount[a] * es);
+        if (p) {
+          auto tw = twiddles<double>(dims[a]);
+          auto tn = tan_table<double>(dims[a], tcount[a]);
+          CK(cudaMemcpy(h->tw[p][a], tw.data(), tw.size() * es, cudaMemcpyHostToDevice));
+          CK(cudaMemcpy(h->tn[p][a], tn.data(), tn.size() * es, cudaMemcpyHostToDevice));
+        } else {
+          auto tw = twiddles<float>(dims[a]);
+          auto tn = tan_table<float>(dims[a], tcount[a]);
+          CK(cudaMemcpy(h->tw[p][a], tw.data(), tw.size() * es, cudaMemcpyHostToDevice));
+          CK(cudaMemcpy(h->tn[p][a], tn.data(), tn.size() * es, cudaMemcpyHostToDevice));
+        }
+      }
+    CKR((set_kernel_attrs<double, double>(SMEM_LIMIT)));
+    CKR((set_kernel_attrs<float, float>(SMEM_LIMIT)));
+    CKR((set_kernel_attrs<double, float>(SMEM_LIMIT)));
+    void **fields[] = {&h->eps, &h->sig, &h->sig_old, &h->eps_old, &h->dfl, &h->guess, &h->b,
+                       &h->kr[0], &h->kr[1], &h->kr[2], &h->kr[3], &h->kr[4], &h->kr[5]};
+    for (void **f : fields) {
+      ALLOC(*f, field_bytes(h, 6));
+      CK(cudaMemset(*f, 0, field_bytes(h, 6)));
+    }
+    ALLOC(h->spec, (size_t)6 * h->S * 16);  // sized for double-precision transforms
+    ALLOC(h->partials, (size_t)MAX_PARTIAL_BLOCKS * 21 * sizeof(double));
+    ALLOC(h->tickets, 16 * sizeof(unsigned int));
+    CK(cudaMemset(h->tickets, 0, 16 * sizeof(unsigned int)));
+    ALLOC(h->results, 64 * sizeof(double));
+    CK(cudaMemset(h->results, 0, 64 * sizeof(double)));
+    ALLOC(h->st, sizeof(MinresState));
+    ALLOC(h->citers, 4 * sizeof(int));
+    ALLOC(h->dparams, SSFFT_MAX_PHASES * sizeof(PhaseParams));
+    CK(cudaMallocHost((void **)&h->h_results, 64 * sizeof(double)));
+    CK(cudaMallocHost((void **)&h->h_st, sizeof(MinresState)));
+    CK(cudaMallocHost((void **)&h->h_cint, 4 * sizeof(int)));
+    h->cfail = h->citers + 1;
+    return 0;
+  };
+  rc = body();
+  if (rc) {
+    free_handle(h);
+    return rc;
+  }
+  *out = h;
+  return 0;
+}
+
+extern "C" int ssfft_destroy(ssfft_handle *h) {
+  if (!h) return 0;
+  cudaSetDevice(h->cfg.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_handle(h);
+  return 0;
+}
+
+static int check_phase(ssfft_handle *h, int phase) {
+  if (!h) return fail(SSFFT_E_INVALID, "null handle");
+  if (phase < 0 || phase >= SSFFT_MAX_PHASES) return fail(SSFFT_E_INVALID, "phase index out of range");
+  if (h->micro_set) return fail(SSFFT_E_INVALID, "phases must be set before the microstructure");
+  return 0;
+}
+
+extern "C" int ssfft_set_phase_elastic(ssfft_handle *h, int phase, const double stiffness[36]) {
+  CKR(check_phase(h, phase));
+  PhaseParams &P = h->hparams[phase];
+  memset(&P, 0, sizeof(P));
+  P.kind = PHASE_ELASTIC;
+  memcpy(P.C, stiffness, 36 * sizeof(double));
+  P.latent = 1.0;
+  h->phase_set[phase] = true;
+  return 0;
+}
+
+extern "C" int ssfft_set_phase_evp(ssfft_handle *h, int phase, const double stiffness[36],
+                                   int n_slip, const double *schmid, double reference_slip_rate,
+                                   double rate_exponent, double slip_resistance, int hardening,
+                                   const double *hardening_props, int n_props,
+                                   double latent_ratio) {
+  CKR(check_phase(h, phase));
+  if (n_slip < 1 || n_slip > SSFFT_MAX_SLIP)
+    return fail(SSFFT_E_UNSUPPORTED, "number of slip systems must be 1..12");
+  if (hardening < 0 || hardening > 3) return fail(SSFFT_E_INVALID, "unknown hardening law");
+  if (n_props < 0 || n_props > 4) return fail(SSFFT_E_INVALID, "at most 4 hardening properties");
+  PhaseParams &P = h->hparams[phase];
+  memset(&P, 0, sizeof(P));
+  P.kind = PHASE_EVP;
+  P.nslip = n_slip;
+  P.hardening = hardening;
+  memcpy(P.C, stiffness, 36 * sizeof(double));
+  if (!inv6(P.C, P.Cinv)) return fail(SSFFT_E_INVALID, "EVP stiffness is singular");
+  // the packed M uses the upper triangle of C^-1; symmetrise against round-off
+  for (int i = 0; i < 6; ++i)
+    for (int j = i + 1; j < 6; ++j) {
+      const double s = 0.5 * (P.Cinv[i * 6 + j] + P.Cinv[j * 6 + i]);
+      P.Cinv[i * 6 + j] = P.Cinv[j * 6 + i] = s;
+    }
+  memcpy(P.P, schmid, (size_t)n_slip * 6 * sizeof(double));
+  P.gdot0 = reference_slip_rate;
+  P.n = rate_exponent;
+  P.g0 = slip_resistance;
+  P.latent = latent_ratio;
+  for (int k = 0; k < n_props; ++k) P.props[k] = hardening_props[k];
+  // directional modulus along x: 1 / (C^-1)_00 (elastic_viscoplastic.py:32-34)
+  P.E_ref = 1.0 / P.Cinv[0];
+  h->phase_set[phase] = true;
+  return 0;
+}
+
+template <typename T> static void build_ktab(const ssfft_handle *h, const std::vector<double> &Rm,
+                                             const std::vector<int> &gid_orient,
+                                             const std::vector<int> &gid_phase,
+                                             std::vector<T> &tab) {
+  const int n = (int)gid_orient.size();
+  tab.assign((size_t)n * 21, (T)0);
+  for (int g = 0; g < n; ++g) {
+    const double *R = &Rm[(size_t)gid_orient[g] * 36];
+    const double *C = h->hparams[gid_phase[g]].C;
+    double CR[36];
+    for (int i = 0; i < 6; ++i)
+      for (int b = 0; b < 6; ++b) {
+        double acc = 0.0;
+        for (int j = 0; j < 6; ++j) acc += C[i * 6 + j] * R[j * 6 + b];
+        CR[i * 6 + b] = acc;
+      }
+    for (int a = 0; a < 6; ++a)
+      for (int b = a; b < 6; ++b) {
+        double acc = 0.0;
+        for (int i = 0; i < 6; ++i) acc += R[i * 6 + a] * CR[i * 6 + b];
+        tab[(size_t)g * 21 + sym_idx(a, b)] = (T)acc;
+      }
+  }
+}
+
+// Mandel form of a rotation (materialite/tensor.py:1668-1700).
+static void rotation_mandel(const double *R, double *M) {
+  const double r2 = SQRT2_D;
+  auto r = [&](int i, int j) { return R[i * 3 + j]; };
+  const int pr[3][2] = {{1, 2}, {0, 2}, {0, 1}};
+  for (int a = 0; a < 3; ++a) {
+    for (int b = 0; b < 3; ++b) M[a * 6 + b] = r(a, b) * r(a, b);
+    for (int s = 0; s < 3; ++s) M[a * 6 + 3 + s] = r2 * r(a, pr[s][0]) * r(a, pr[s][1]);
+  }
+  for (int s = 0; s < 3; ++s) {
+    const int i = pr[s][0], j = pr[s][1];
+    for (int b = 0; b < 3; ++b) M[(3 + s) * 6 + b] = r2 * r(i, b) * r(j, b);
+    for (int t = 0; t < 3; ++t) {
+      const int k = pr[t][0], l = pr[t][1];
+      M[(3 + s) * 6 + 3 + t] = r(i, k) * r(j, l) + r(i, l) * r(j, k);
+    }
+  }
+}
+
+extern "C" int ssfft_set_microstructure(ssfft_handle *h, int n_orient, const double *rotations,
+                                        const int32_t *orient_of_point,
+                                        const int32_t *phase_of_point) {
+  if (!h) return fail(SSFFT_E_INVALID, "null handle");
+  if (h->micro_set) return fail(SSFFT_E_INVALID, "microstructure already set");
+  if (n_orient < 1 || !rotations || !orient_of_point)
+    return fail(SSFFT_E_INVALID, "rotations and orientation indices are required");
+  CK(cudaSetDevice(h->cfg.device));
+  const long long V = h->V;
+  int max_phase = 0;
+  for (long long v = 0; v < V; ++v) {
+    const int o = orient_of_point[v];
+    const int p = phase_of_point ? phase_of_point[v] : 0;
+    if (o < 0 || o >= n_orient) return fail(SSFFT_E_INVALID, "orientation index out of range");
+    if (p < 0 || p >= SSFFT_MAX_PHASES || !h->phase_set[p])
+      return fail(SSFFT_E_INVALID, "point refers to an undefined phase");
+    max_phase = std::max(max_phase, p);
+  }
+  h->any_evp = false;
+  h->nslip_max = 0;
+  for (int p = 0; p < SSFFT_MAX_PHASES; ++p)
+    if (h->phase_set[p] && h->hparams[p].kind == PHASE_EVP) {
+      h->any_evp = true;
+      h->nslip_max = std::max(h->nslip_max, h->hparams[p].nslip);
+    }
+  h->voxel_mode = h->any_evp;
+  h->n_orient = n_orient;
+  std::vector<double> Rm((size_t)n_orient * 36);
+  for (int o = 0; o < n_orient; ++o) rotation_mandel(rotations + (size_t)o * 9, &Rm[(size_t)o * 36]);
+  ALLOC(h->rm_tab, Rm.size() * sizeof(double));
+  CK(cudaMemcpy(h->rm_tab, Rm.data(), Rm.size() * sizeof(double), cudaMemcpyHostToDevice));
+  ALLOC(h->orient, V * sizeof(int32_t));
+  CK(cudaMemcpy(h->orient, orient_of_point, V * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (phase_of_point) {
+    ALLOC(h->phase, V * sizeof(int32_t));
+    CK(cudaMemcpy(h->phase, phase_of_point, V * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpy(h->dparams, h->hparams, sizeof(h->hparams), cudaMemcpyHostToDevice));
+  if (!h->voxel_mode) {
+    // tangent table over the distinct (orientation, phase) pairs present
+    std::vector<int> key_to_gid((size_t)n_orient * (max_phase + 1), -1);
+    std::vector<int> g_or, g_ph;
+    std::vector<int32_t> gid(V);
+    for (long long v = 0; v < V; ++v) {
+      const int o = orient_of_point[v], p = phase_of_point ? phase_of_point[v] : 0;
+      int &slot = key_to_gid[(size_t)p * n_orient + o];
+      if (slot < 0) {
+        slot = (int)g_or.size();
+        g_or.push_back(o);
+        g_ph.push_back(p);
+      }
+      gid[v] = slot;
+    }
+    h->n_gid = (int)g_or.size();
+    ALLOC(h->gid, V * sizeof(int32_t));
+    CK(cudaMemcpy(h->gid, gid.data(), V * sizeof(int32_t), cudaMemcpyHostToDevice));
+    if (h->fp64) {
+      std::vector<double> tab;
+      build_ktab<double>(h, Rm, g_or, g_ph, tab);
+      ALLOC(h->ktab, tab.size() * sizeof(double));
+      CK(cudaMemcpy(h->ktab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> tab;
+      build_ktab<float>(h, Rm, g_or, g_ph, tab);
+      ALLOC(h->ktab, tab.size() * sizeof(float));
+      CK(cudaMemcpy(h->ktab, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+  } else {
+    ALLOC(h->kvox, field_bytes(h, 21));
+    ALLOC(h->kvox_old, field_bytes(h, 21));
+    const int S = h->nslip_max;
+    ALLOC(h->g_buf[0], (size_t)S * V * 8);
+    ALLOC(h->g_buf[1], (size_t)S * V * 8);
+    ALLOC(h->g_old, (size_t)S * V * 8);
+    ALLOC(h->gam_old, (size_t)S * V * 8);
+    ALLOC(h->gam_trial, (size_t)S * V * 8);
+    ALLOC(h->ep_old, (size_t)6 * V * 8);
+    ALLOC(h->ep_trial, (size_t)6 * V * 8);
+    ALLOC(h->Gam_old, (size_t)V * 8);
+    ALLOC(h->Gam_trial, (size_t)V * 8);
+  }
+  h->micro_set = true;
+  return ssfft_reset(h);
+}
+
+extern "C" int ssfft_reset(ssfft_handle *h) {
+  if (!h || !h->micro_set) return fail(SSFFT_E_INVALID, "microstructure not set");
+  CK(cudaSetDevice(h->cfg.device));
+  void *fields[] = {h->eps, h->sig, h->sig_old, h->eps_old, h->dfl, h->guess, h->b};
+  for (void *f : fields) CK(cudaMemsetAsync(f, 0, field_bytes(h, 6), h->stream));
+  const long long V = h->V;
+  const int eb = std::max(1, std::min(div_up(V, SSFFT_THREADS), 148 * 16));
+  if (h->voxel_mode) {
+    if (h->fp64)
+      init_kvox_kernel<double><<<eb, SSFFT_THREADS, 0, h->stream>>>(
+          V, h->phase, h->orient, h->dparams, h->rm_tab, (double *)h->kvox);
+    else
+      init_kvox_kernel<float><<<eb, SSFFT_THREADS, 0, h->stream>>>(
+          V, h->phase, h->orient, h->dparams, h->rm_tab, (float *)h->kvox);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->kvox_old, h->kvox, field_bytes(h, 21), cudaMemcpyDeviceToDevice,
+                       h->stream));
+  }
+  if (h->any_evp) {
+    const int S = h->nslip_max;
+    evp_init_kernel<<<eb, SSFFT_THREADS, 0, h->stream>>>(V, S, h->phase, h->dparams,
+                                                         h->g_buf[0], h->g_buf[1], h->g_old);
+    CK(cudaGetLastError());
+    CK(cudaMemsetAsync(h->gam_old, 0, (size_t)S * V * 8, h->stream));
+    CK(cudaMemsetAsync(h->gam_trial, 0, (size_t)S * V * 8, h->stream));
+    CK(cudaMemsetAsync(h->ep_old, 0, (size_t)6 * V * 8, h->stream));
+    CK(cudaMemsetAsync(h->ep_trial, 0, (size_t)6 * V * 8, h->stream));
+    CK(cudaMemsetAsync(h->Gam_old, 0, (size_t)V * 8, h->stream));
+    CK(cudaMemsetAsync(h->Gam_trial, 0, (size_t)V * 8, h->stream));
+    h->g_cur = 0;
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+extern "C" int ssfft_step(ssfft_handle *h, const ssfft_step_in *in, ssfft_step_out *out) {
+  if (!h || !in || !out) return fail(SSFFT_E_INVALID, "null argument");
+  if (!h->micro_set) return fail(SSFFT_E_INVALID, "microstructure not set");
+  if (!(in->dt > 0.0)) return fail(SSFFT_E_INVALID, "time increment must be positive");
+  CK(cudaSetDevice(h->cfg.device));
+  return h->fp64 ? step_impl<double>(h, in, out) : step_impl<float>(h, in, out);
+}
+
+extern "C" int ssfft_commit(ssfft_handle *h, double fluctuation_scale) {
+  if (!h || !h->micro_set) return fail(SSFFT_E_INVALID, "microstructure not set");
+  CK(cudaSetDevice(h->cfg.device));
+  const size_t f6 = field_bytes(h, 6);
+  CK(cudaMemcpyAsync(h->sig_old, h->sig, f6, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->eps_old, h->eps, f6, cudaMemcpyDeviceToDevice, h->stream));
+  if (h->voxel_mode)
+    CK(cudaMemcpyAsync(h->kvox_old, h->kvox, field_bytes(h, 21), cudaMemcpyDeviceToDevice,
+                       h->stream));
+  if (h->any_evp) {
+    const size_t V = (size_t)h->V, S = (size_t)h->nslip_max;
+    CK(cudaMemcpyAsync(h->g_old, h->g_buf[h->g_cur], S * V * 8, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->gam_old, h->gam_trial, S * V * 8, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->ep_old, h->ep_trial, 6 * V * 8, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->Gam_old, h->Gam_trial, V * 8, cudaMemcpyDeviceToDevice, h->stream));
+  }
+  return ssfft_scale_fluctuation(h, fluctuation_scale);
+}
+
+extern "C" int ssfft_scale_fluctuation(ssfft_handle *h, double factor) {
+  if (!h || !h->micro_set) return fail(SSFFT_E_INVALID, "microstructure not set");
+  CK(cudaSetDevice(h->cfg.device));
+  const long long n = 6 * h->V;
+  const int eb = std::max(1, std::min(div_up(n, SSFFT_THREADS), 148 * 16));
+  if (factor != 1.0) {
+    if (h->fp64)
+      scale_kernel<double><<<eb, SSFFT_THREADS, 0, h->stream>>>(n, (double *)h->dfl, factor);
+    else
+      scale_kernel<float><<<eb, SSFFT_THREADS, 0, h->stream>>>(n, (float *)h->dfl, factor);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+extern "C" int ssfft_num_slip(ssfft_handle *h) { return h ? h->nslip_max : 0; }
+
+extern "C" int ssfft_get_field(ssfft_handle *h, int field, double *dst, int to_host) {
+  if (!h || !dst) return fail(SSFFT_E_INVALID, "null argument");
+  if (!h->micro_set) return fail(SSFFT_E_INVALID, "microstructure not set");
+  CK(cudaSetDevice(h->cfg.device));
+  const long long V = h->V;
+  int width = 6;
+  const void *src = nullptr;
+  bool is_double = false;
+  switch (field) {
+    case SSFFT_FIELD_STRESS: src = h->sig; break;
+    case SSFFT_FIELD_STRAIN: src = h->eps; break;
+    case SSFFT_FIELD_RESIDUAL: src = h->b; break;
+    case SSFFT_FIELD_SLIP_RESISTANCES:
+    case SSFFT_FIELD_SLIP_SHEAR_STRAINS:
+    case SSFFT_FIELD_PLASTIC_STRAINS:
+      if (!h->any_evp) return fail(SSFFT_E_INVALID, "no crystal-plasticity phase in this solve");
+      is_double = true;
+      if (field == SSFFT_FIELD_SLIP_RESISTANCES) {
+        src = h->g_buf[h->g_cur];
+        width = h->nslip_max;
+      } else if (field == SSFFT_FIELD_SLIP_SHEAR_STRAINS) {
+        src = h->gam_trial;
+        width = h->nslip_max;
+      }
+      break;
+    default: return fail(SSFFT_E_INVALID, "unknown field id");
+  }
+  double *ddst = dst;
+  if (to_host) ALLOC(ddst, (size_t)V * width * sizeof(double));
+  const int eb = std::max(1, std::min(div_up(V * width, SSFFT_THREADS), 148 * 16));
+  if (field == SSFFT_FIELD_PLASTIC_STRAINS) {
+    plastic_to_specimen_kernel<<<eb, SSFFT_THREADS, 0, h->stream>>>(V, h->ep_old, h->orient,
+                                                                     h->rm_tab, ddst);
+  } else if (is_double || h->fp64) {
+    to_point_major_kernel<double><<<eb, SSFFT_THREADS, 0, h->stream>>>(V, width,
+                                                                       (const double *)src, ddst);
+  } else {
+    to_point_major_kernel<float><<<eb, SSFFT_THREADS, 0, h->stream>>>(V, width,
+                                                                      (const float *)src, ddst);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && to_host) {
+    e = cudaMemcpyAsync(dst, ddst, (size_t)V * width * sizeof(double), cudaMemcpyDeviceToHost,
+                        h->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (to_host) cudaFree(ddst);
+  if (e != cudaSuccess) return fail(SSFFT_E_CUDA, std::string("get_field: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+template <typename T> static int apply_projection_dev(ssfft_handle *h, const T *in, T *out) {
+  ProArgs<T> pa{};
+  pa.in = in;
+  EpiArgs<T> ea{};
+  ea.out = out;
+  return launch_projector<T, T, PRO_INPUT, EPI_STORE>(h, pa, ea, nullptr);
+}
+
+extern "C" int ssfft_apply_projection_device(ssfft_handle *h, const void *in_dev, void *out_dev) {
+  if (!h || !in_dev || !out_dev) return fail(SSFFT_E_INVALID, "null argument");
+  CK(cudaSetDevice(h->cfg.device));
+  if (h->fp64)
+    CKR(apply_projection_dev<double>(h, (const double *)in_dev, (double *)out_dev));
+  else
+    CKR(apply_projection_dev<float>(h, (const float *)in_dev, (float *)out_dev));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+extern "C" int ssfft_apply_projection(ssfft_handle *h, const double *in_host, double *out_host) {
+  if (!h || !in_host || !out_host) return fail(SSFFT_E_INVALID, "null argument");
+  CK(cudaSetDevice(h->cfg.device));
+  const long long V = h->V;
+  double *tmp = nullptr;
+  ALLOC(tmp, (size_t)V * 6 * sizeof(double));
+  const int eb = std::max(1, std::min(div_up(V * 6, SSFFT_THREADS), 148 * 16));
+  int rc = 0;
+  cudaError_t e = cudaMemcpyAsync(tmp, in_host, (size_t)V * 6 * sizeof(double),
+                                  cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) {
+    if (h->fp64) {
+      from_point_major_kernel<double><<<eb, SSFFT_THREADS, 0, h->stream>>>(V, tmp, (double *)h->kr[0]);
+      rc = apply_projection_dev<double>(h, (const double *)h->kr[0], (double *)h->kr[1]);
+      to_point_major_kernel<double><<<eb, SSFFT_THREADS, 0, h->stream>>>(V, 6, (const double *)h->kr[1], tmp);
+    } else {
+      from_point_major_kernel<float><<<eb, SSFFT_THREADS, 0, h->stream>>>(V, tmp, (float *)h->kr[0]);
+      rc = apply_projection_dev<float>(h, (const float *)h->kr[0], (float *)h->kr[1]);
+      to_point_major_kernel<float><<<eb, SSFFT_THREADS, 0, h->stream>>>(V, 6, (const float *)h->kr[1], tmp);
+    }
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && rc == 0)
+    e = cudaMemcpyAsync(out_host, tmp, (size_t)V * 6 * sizeof(double), cudaMemcpyDeviceToHost,
+                        h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(tmp);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(SSFFT_E_CUDA, std::string("apply_projection: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+extern "C" int ssfft_stats(ssfft_handle *h, double *step_seconds, int64_t *kernel_launches) {
+  if (!h) return fail(SSFFT_E_INVALID, "null handle");
+  if (step_seconds) *step_seconds = h->last_step_seconds;
+  if (kernel_launches) *kernel_launches = h->launches;
+  return 0;
+}
+
+extern "C" int ssfft_timer(ssfft_handle *h, int start, double *seconds) {
+  if (!h) return fail(SSFFT_E_INVALID, "null handle");
+  CK(cudaSetDevice(h->cfg.device));
+  if (start) {
+    CK(cudaEventRecord(h->tev0, h->stream));
+    return 0;
+  }
+  CK(cudaEventRecord(h->tev1, h->stream));
+  CK(cudaEventSynchronize(h->tev1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, h->tev0, h->tev1));
+  if (seconds) *seconds = ms * 1e-3;
+  return 0;
+}
+
+template <typename T> static int profile_impl(ssfft_handle *h, int reps, double *sec) {
+  const long long n = 6 * h->V;
+  T *R1 = (T *)h->kr[0], *R2 = (T *)h->kr[1], *W = (T *)h->kr[2], *W1 = (T *)h->kr[3],
+    *W2 = (T *)h->kr[4], *X = (T *)h->kr[5];
+  // a live MINRES state on the residual of the current stress (never marked done); call
+  // after a solve so that the stress field is not uniform
+  const double zero[6] = {0, 0, 0, 0, 0, 0};
+  CKR(residual<T>(h, zero));
+  minres_init_kernel<T><<<h->red_blocks, SSFFT_THREADS, 0, h->stream>>>(
+      (const T *)h->b, R1, R2, X, W, W2, n, h->st, 0.0, (long long)1 << 60, h->partials,
+      h->tickets + TK_INIT);
+  CK(cudaGetLastError());
+  Grid<T> g = make_grid<T>(h);
+  cplx<T> *spec = (cplx<T> *)h->spec;
+  const size_t cs = sizeof(cplx<T>);
+  const size_t sz = (6 * (size_t)h->lz * h->nz + h->nz) * cs;
+  const size_t sy = (2 * (size_t)h->ky * h->ny + h->ny) * cs;
+  const size_t sx = (12 * (size_t)h->kx * h->nx + h->nx) * cs;
+  const int nzb = div_up((long long)h->nx * h->ny, h->lz);
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int r = 0; r < reps; ++r) {
+    ProArgs<T> pa{};
+    pa.in = R2;
+    pa.gid = h->gid;
+    pa.ktab = (const T *)h->ktab;
+    pa.kvox = (const T *)h->kvox;
+    pa.st = h->st;
+    EpiArgs<T> ea{};
+    ea.out = R1;
+    ea.r2 = R2;
+    ea.st = h->st;
+    ea.partials = h->partials;
+    ea.ticket = h->tickets + TK_ZINV;
+    CK(cudaEventRecord(h->pev[0], h->stream));
+    if (h->voxel_mode)
+      zfwd_kernel<T, T, PRO_TANGENT_VOXEL><<<nzb, SSFFT_THREADS, sz, h->stream>>>(g, pa, spec);
+    else
+      zfwd_kernel<T, T, PRO_TANGENT_TABLE><<<nzb, SSFFT_THREADS, sz, h->stream>>>(g, pa, spec);
+    CK(cudaEventRecord(h->pev[1], h->stream));
+    ypass_kernel<T, false><<<dim3(div_up(h->hz, h->ky), h->nx, 6), SSFFT_THREADS, sy,
+                             h->stream>>>(g, spec, h->st);
+    CK(cudaEventRecord(h->pev[2], h->stream));
+    xpass_kernel<T><<<dim3(div_up(h->hz, h->kx), h->ny), SSFFT_THREADS, sx, h->stream>>>(
+        g, spec, h->st);
+    CK(cudaEventRecord(h->pev[3], h->stream));
+    ypass_kernel<T, true><<<dim3(div_up(h->hz, h->ky), h->nx, 6), SSFFT_THREADS, sy,
+                            h->stream>>>(g, spec, h->st);
+    CK(cudaEventRecord(h->pev[4], h->stream));
+    zinv_kernel<T, T, EPI_MINRES><<<nzb, SSFFT_THREADS, sz, h->stream>>>(g, ea, spec);
+    CK(cudaEventRecord(h->pev[5], h->stream));
+    minres_upd1_kernel<T><<<h->red_blocks, SSFFT_THREADS, 0, h->stream>>>(
+        R1, R2, n, h->st, h->partials, h->tickets + TK_UPD1);
+    CK(cudaEventRecord(h->pev[6], h->stream));
+    std::swap(R1, R2);
+    minres_upd2_kernel<T><<<h->red_blocks, SSFFT_THREADS, 0, h->stream>>>(
+        R1, W2, W, W1, X, n, h->st, h->partials, h->tickets + TK_UPD2);
+    CK(cudaEventRecord(h->pev[7], h->stream));
+    T *old_w1 = W1;
+    W1 = W2;
+    W2 = W;
+    W = old_w1;
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(h->pev[7]));
+    for (int k = 0; k < 7; ++k) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, h->pev[k], h->pev[k + 1]));
+      acc[k] += ms * 1e-3;
+    }
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, h->pev[0], h->pev[7]));
+    acc[7] += ms * 1e-3;
+  }
+  for (int k = 0; k < 8; ++k) sec[k] = acc[k] / reps;
+  h->launches += 7LL * reps;
+  return 0;
+}
+
+extern "C" int ssfft_profile_krylov(ssfft_handle *h, int reps, double seconds[8]) {
+  if (!h || !seconds || reps < 1) return fail(SSFFT_E_INVALID, "bad argument");
+  if (!h->micro_set) return fail(SSFFT_E_INVALID, "microstructure not set");
+  CK(cudaSetDevice(h->cfg.device));
+  return h->fp64 ? profile_impl<double>(h, reps, seconds) : profile_impl<float>(h, reps, seconds);
+}

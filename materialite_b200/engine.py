@@ -1,0 +1,270 @@
+"""Array-level driver of libssfft: one solver handle per RVE and the time loop of
+materialite's SmallStrainFFT.run (materialite/models/small_strain_fft/small_strain_fft.py:
+60-279).
+
+``SmallStrainFFT`` (the drop-in class) and the serving loop both call ``solve``; the
+per-step Newton/Krylov work runs on the GPU inside ``ssfft_step``.
+"""
+
+import ctypes
+import math
+from collections import defaultdict
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _native as nat
+
+
+@dataclass
+class PhaseSpec:
+    """One constitutive phase: ``kind`` is "elastic" or "evp"; stiffness is a 6x6 Mandel
+    matrix.  EVP phases carry Mandel Schmid tensors (S,6) and the parameters of
+    ElasticViscoplastic (elastic_viscoplastic.py:21-50)."""
+    kind: str
+    stiffness: np.ndarray
+    schmid: Optional[np.ndarray] = None
+    reference_slip_rate: float = 1.0
+    rate_exponent: float = 1.0
+    slip_resistance: float = 1.0
+    hardening: str = "perfect_plasticity"
+    hardening_props: tuple = ()
+    latent_ratio: float = 1.0
+
+
+def hardening_props_vector(kind, props):
+    """Order the hardening-property dict as libssfft expects (hardening_laws.py:18-90)."""
+    props = props or {}
+    if kind == "perfect_plasticity":
+        return ()
+    if kind == "linear":
+        return (float(props["hardening_rate"]),)
+    if kind == "voce":
+        return (float(props["tau_1"]), float(props["theta_0"]), float(props["theta_1"]))
+    if kind == "armstrong_frederick":
+        return (float(props["direct_hardening"]), float(props["dynamic_recovery"]))
+    raise ValueError(f"unknown hardening law {kind}")
+
+
+def unique_rotations(R):
+    """Deduplicate per-point rotation matrices: returns (table (n,3,3), index (V,))."""
+    R = np.ascontiguousarray(np.asarray(R, dtype=np.float64).reshape(-1, 9))
+    table, index = np.unique(R, axis=0, return_inverse=True)
+    return table.reshape(-1, 3, 3), index.reshape(-1).astype(np.int32)
+
+
+class SolverHandle:
+    """Owns one libssfft handle (device buffers of one RVE grid)."""
+
+    def __init__(self, dims, stress_mask, precision="mixed", global_tolerance=1.0e-3,
+                 strain_correction_tolerance=1.0e-2, linear_solver_tolerance=1.0e-5,
+                 max_newton_iterations=100, max_krylov_iterations=0, device=0):
+        self.lib = nat.load_library()
+        cfg = nat.SsfftConfig()
+        for d in range(3):
+            cfg.n[d] = int(dims[d])
+        cfg.precision = nat.SSFFT_FP64 if precision == "fp64" else nat.SSFFT_MIXED
+        cfg.device = int(device)
+        cfg.max_newton_iterations = int(max_newton_iterations)
+        cfg.max_krylov_iterations = int(max_krylov_iterations)
+        cfg.global_tolerance = float(global_tolerance)
+        cfg.strain_correction_tolerance = float(strain_correction_tolerance)
+        cfg.linear_solver_tolerance = float(linear_solver_tolerance)
+        for c in range(6):
+            cfg.stress_mask[c] = float(stress_mask[c])
+        self.cfg = cfg
+        self.dims = tuple(int(d) for d in dims)
+        self.V = int(np.prod(self.dims))
+        self.precision = precision
+        h = ctypes.c_void_p()
+        nat.check(self.lib.ssfft_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self.nslip = 0
+        self.phases = []
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.ssfft_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_phases(self, phases):
+        self.phases = list(phases)
+        for i, p in enumerate(self.phases):
+            C = np.ascontiguousarray(p.stiffness, dtype=np.float64).reshape(36)
+            if p.kind == "elastic":
+                nat.check(self.lib.ssfft_set_phase_elastic(self.h, i, nat.as_double_ptr(C)))
+            elif p.kind == "evp":
+                P = np.ascontiguousarray(p.schmid, dtype=np.float64).reshape(-1, 6)
+                props = np.ascontiguousarray(
+                    list(hardening_props_vector(p.hardening, p.hardening_props)) + [0.0],
+                    dtype=np.float64)
+                nprops = len(hardening_props_vector(p.hardening, p.hardening_props))
+                nat.check(self.lib.ssfft_set_phase_evp(
+                    self.h, i, nat.as_double_ptr(C), P.shape[0], nat.as_double_ptr(P),
+                    float(p.reference_slip_rate), float(p.rate_exponent),
+                    float(p.slip_resistance), nat.HARDENING_IDS[p.hardening],
+                    nat.as_double_ptr(props), nprops, float(p.latent_ratio)))
+                self.nslip = max(self.nslip, P.shape[0])
+            else:
+                raise ValueError(f"unknown phase kind {p.kind}")
+
+    def set_microstructure(self, rotations, orient_of_point, phase_of_point=None):
+        R = np.ascontiguousarray(rotations, dtype=np.float64).reshape(-1, 9)
+        o = np.ascontiguousarray(orient_of_point, dtype=np.int32).reshape(-1)
+        if o.size != self.V:
+            raise ValueError("orientation index must have one entry per point")
+        ph = None
+        if phase_of_point is not None:
+            ph = np.ascontiguousarray(phase_of_point, dtype=np.int32).reshape(-1)
+            if ph.size != self.V:
+                raise ValueError("phase index must have one entry per point")
+        nat.check(self.lib.ssfft_set_microstructure(
+            self.h, R.shape[0], nat.as_double_ptr(R), nat.as_int_ptr(o),
+            nat.as_int_ptr(ph) if ph is not None else None))
+
+    def reset(self):
+        nat.check(self.lib.ssfft_reset(self.h))
+
+    def step(self, dE, dS, Sbar, dt, summed_vm, step_id, reset):
+        si = nat.SsfftStepIn()
+        for c in range(6):
+            si.strain_increment[c] = float(dE[c])
+            si.stress_increment[c] = float(dS[c])
+            si.mean_applied_stress[c] = float(Sbar[c])
+        si.dt = float(dt)
+        si.summed_von_mises_stress = float(summed_vm)
+        si.time_step_id = int(step_id)
+        si.reset_fluctuation = int(bool(reset))
+        so = nat.SsfftStepOut()
+        nat.check(self.lib.ssfft_step(self.h, ctypes.byref(si), ctypes.byref(so)))
+        if so.status != 0:
+            raise nat.SsfftError(so.status, "non-finite equilibrium error")
+        return so
+
+    def commit(self, scale):
+        nat.check(self.lib.ssfft_commit(self.h, float(scale)))
+
+    def scale_fluctuation(self, f):
+        nat.check(self.lib.ssfft_scale_fluctuation(self.h, float(f)))
+
+    def field(self, name):
+        width = self.nslip if name in ("slip_resistances", "slip_system_shear_strains") else 6
+        out = np.empty((self.V, width), dtype=np.float64)
+        nat.check(self.lib.ssfft_get_field(self.h, nat.FIELD_IDS[name], nat.as_double_ptr(out), 1))
+        return out
+
+    def apply_projection(self, tau):
+        tau = np.ascontiguousarray(tau, dtype=np.float64).reshape(self.V, 6)
+        out = np.empty_like(tau)
+        nat.check(self.lib.ssfft_apply_projection(self.h, nat.as_double_ptr(tau),
+                                                  nat.as_double_ptr(out)))
+        return out.ravel()
+
+    def timer_start(self):
+        nat.check(self.lib.ssfft_timer(self.h, 1, None))
+
+    def timer_stop(self):
+        s = ctypes.c_double()
+        nat.check(self.lib.ssfft_timer(self.h, 0, ctypes.byref(s)))
+        return s.value
+
+    def profile_krylov(self, reps=20):
+        out = np.zeros(8)
+        nat.check(self.lib.ssfft_profile_krylov(self.h, int(reps), nat.as_double_ptr(out)))
+        return out
+
+    def stats(self):
+        s = ctypes.c_double()
+        n = ctypes.c_int64()
+        nat.check(self.lib.ssfft_stats(self.h, ctypes.byref(s), ctypes.byref(n)))
+        return s.value, n.value
+
+
+@dataclass
+class SolveStats:
+    steps: int = 0
+    cutbacks: int = 0
+    newton_iterations: list = field(default_factory=list)
+    krylov_iterations: list = field(default_factory=list)
+    device_seconds: float = 0.0
+
+
+def solve(handle, dstrain, dstress, stress, end_time=1.0, initial_time_increment=None,
+          max_time_increment=None, min_time_increment=1.0e-9, start_time=0.0,
+          output_times=None, output_variables=None, stats=None, outputs_hook=None):
+    """The time loop of SmallStrainFFT.run (small_strain_fft.py:73-246) over a prepared
+    handle.  ``dstrain``, ``dstress`` and ``stress`` are the LoadSchedule closures
+    returning Mandel 6-vectors.  Returns (final_outputs, history) where history maps each
+    output name to the list of values at ``output_times``."""
+    dt = end_time if initial_time_increment is None else initial_time_increment
+    dt_max = dt if max_time_increment is None else max_time_increment
+    t = start_time
+    t_tol = min_time_increment / 2.0
+    if output_times is not None:
+        out_idx = 0
+        output_times = np.append(output_times, np.inf)
+        next_out = output_times[0]
+    else:
+        next_out = np.inf
+    history = defaultdict(list)
+    old_max_inc = 0.0
+    summed_vm = 0.0
+    step_id = 0
+    handle.reset()
+    while t < end_time - t_tol:
+        dE = np.asarray(dstrain(t, dt), dtype=np.float64).reshape(6)
+        dS = np.asarray(dstress(t, dt), dtype=np.float64).reshape(6)
+        Sbar = np.asarray(stress(t, dt), dtype=np.float64).reshape(6)
+        max_inc = dE[np.argmax(np.abs(dE))]
+        reset = max_inc * old_max_inc < 0.0
+        out = handle.step(dE, dS, Sbar, dt, summed_vm, step_id, reset)
+        if stats is not None:
+            stats.newton_iterations.append(out.newton_iterations)
+            stats.krylov_iterations.append(out.krylov_iterations)
+            stats.device_seconds += handle.stats()[0]
+        if out.converged:
+            handle.commit(1.0)
+            summed_vm += out.mean_von_mises_stress
+            old_max_inc = max_inc
+            step_id += 1
+            t += dt
+            if t >= next_out - t_tol:
+                if outputs_hook is not None:
+                    outputs_hook(history, handle, output_variables)
+                else:
+                    _collect(history, handle, output_variables)
+                out_idx += 1
+                next_out = output_times[out_idx]
+            # _get_new_time_increment (small_strain_fft.py:266-279)
+            fixed = min(next_out - t, end_time - t)
+            new_dt = min(dt_max, fixed,
+                         dt * 2.0 if out.max_constitutive_iterations < 11 else dt)
+            handle.scale_fluctuation(new_dt / dt)
+            if stats is not None:
+                stats.steps += 1
+            dt = new_dt
+        else:
+            dt = dt / 2.0
+            handle.scale_fluctuation(0.5)
+            if stats is not None:
+                stats.cutbacks += 1
+            if dt < min_time_increment:
+                raise ValueError("min time increment reached")
+    final = {"stress": handle.field("stress"), "strain": handle.field("strain")}
+    for v in (output_variables or []):
+        final[v] = handle.field(v)
+    return final, history
+
+
+def _collect(history, handle, output_variables):
+    for v in (output_variables or []):
+        history[v].append(handle.field(v))
+    history["stress"].append(handle.field("stress"))
+    history["strain"].append(handle.field("strain"))
