@@ -165,6 +165,24 @@ int ssfft_apply_projection(ssfft_handle *h, const double *in_host, double *out_h
  * (6 planes of V values, float or double by precision), on the handle's stream. */
 int ssfft_apply_projection_device(ssfft_handle *h, const void *in_dev, void *out_dev);
 
+/* Allocation-free projection, for callers that cannot allocate device memory (code
+ * that runs where cudaMalloc is unavailable or forbidden: host callbacks, hooks inside
+ * a framework whose allocator owns the device, loops that may not block on an
+ * allocation).  No counterpart in the reference: it is the double-precision
+ * ssfft_apply_projection_device without a handle.
+ *   n, stress_mask : grid and Gamma-hat(0) mask, as in ssfft_config
+ *   in_dev, out_dev: caller-owned device arrays, 6 planes of V doubles each
+ *   stream         : cudaStream_t to launch on (NULL: the legacy default stream);
+ *                    the call waits for it before returning
+ * Its scratch (spectrum and FFT tables) is one file-scope device array of about 13 MB
+ * that every GPU loading the library holds until exit; grids are limited to
+ * nx*ny*(nz/2+1) <= 135168 (64^3) and 1024 points per axis, larger ones are rejected.
+ * The first call on a device (current device) looks up the array's address once; make
+ * it before any stream capture.  All calls share the array: calls that overlap on the
+ * GPU race.  Calls no cudaMalloc, cudaFree or allocating library routine. */
+int ssfft_apply_projection_noalloc(const int32_t n[3], const double stress_mask[6],
+                                   const double *in_dev, double *out_dev, void *stream);
+
 /* Seconds of device time of the last ssfft_step, and kernel launch counters. */
 int ssfft_stats(ssfft_handle *h, double *step_seconds, int64_t *kernel_launches);
 

@@ -38,6 +38,7 @@ EXPORTED_SYMBOLS = [
     "ssfft_reset", "ssfft_step", "ssfft_commit", "ssfft_scale_fluctuation",
     "ssfft_get_field", "ssfft_num_slip", "ssfft_apply_projection",
     "ssfft_apply_projection_device", "ssfft_stats", "ssfft_timer", "ssfft_profile_krylov",
+    "ssfft_apply_projection_noalloc",
 ]
 
 
@@ -124,6 +125,7 @@ def load_library():
     lib.ssfft_stats.argtypes = [P, dp, ctypes.POINTER(ctypes.c_int64)]
     lib.ssfft_timer.argtypes = [P, ctypes.c_int, dp]
     lib.ssfft_profile_krylov.argtypes = [P, ctypes.c_int, dp]
+    lib.ssfft_apply_projection_noalloc.argtypes = [ip, dp, P, P, P]
     for name in EXPORTED_SYMBOLS:
         if name != "ssfft_last_error":
             getattr(lib, name).restype = ctypes.c_int

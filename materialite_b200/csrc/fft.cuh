@@ -18,6 +18,32 @@ struct AxisPlan {
   int rad[SSFFT_MAX_STAGES];    // radix of each stage
 };
 
+// Factor n into stages: radix 8 first, then 4, 2, then odd factors (<= 32).
+static inline bool make_axis_plan(int n, AxisPlan &p) {
+  p.n = n;
+  p.nrad = 0;
+  int m = n;
+  auto push = [&](int r) {
+    if (p.nrad >= SSFFT_MAX_STAGES) return false;
+    p.rad[p.nrad++] = r;
+    m /= r;
+    return true;
+  };
+  while (m % 8 == 0)
+    if (!push(8)) return false;
+  while (m % 4 == 0)
+    if (!push(4)) return false;
+  while (m % 2 == 0)
+    if (!push(2)) return false;
+  for (int f = 3; m > 1; f += 2) {
+    while (m % f == 0) {
+      if (f > SSFFT_MAX_GENERIC_RADIX) return false;
+      if (!push(f)) return false;
+    }
+  }
+  return true;
+}
+
 // Line layout in shared memory: line l starts at
 //   (l / lsub) * lstride_hi + (l % lsub) * lstride_lo
 // and its element j sits at start + j * estride.

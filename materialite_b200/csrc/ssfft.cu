@@ -47,6 +47,11 @@ static int fail(int code, const std::string &msg) {
 
 extern "C" const char *ssfft_last_error(void) { return g_last_error.c_str(); }
 
+// Lets other translation units of the library report through ssfft_last_error().
+__attribute__((visibility("hidden"))) int ssfft_internal_fail(int code, const std::string &msg) {
+  return fail(code, msg);
+}
+
 // ---------------------------------------------------------------------------------------
 // handle
 // ---------------------------------------------------------------------------------------
@@ -103,30 +108,7 @@ struct ssfft_handle {
 // ---------------------------------------------------------------------------------------
 // planning
 // ---------------------------------------------------------------------------------------
-static bool make_plan(int n, AxisPlan &p) {
-  p.n = n;
-  p.nrad = 0;
-  int m = n;
-  auto push = [&](int r) {
-    if (p.nrad >= SSFFT_MAX_STAGES) return false;
-    p.rad[p.nrad++] = r;
-    m /= r;
-    return true;
-  };
-  while (m % 8 == 0)
-    if (!push(8)) return false;
-  while (m % 4 == 0)
-    if (!push(4)) return false;
-  while (m % 2 == 0)
-    if (!push(2)) return false;
-  for (int f = 3; m > 1; f += 2) {
-    while (m % f == 0) {
-      if (f > SSFFT_MAX_GENERIC_RADIX) return false;
-      if (!push(f)) return false;
-    }
-  }
-  return true;
-}
+static bool make_plan(int n, AxisPlan &p) { return make_axis_plan(n, p); }
 
 template <typename T> static std::vector<T> twiddles(int n) {
   std::vector<T> tw(2 * (size_t)n);
