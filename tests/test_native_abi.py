@@ -1,0 +1,72 @@
+"""libssfft loads and exports every entry point include/ssfft.h declares; host-side
+argument validation that needs no GPU."""
+
+import ctypes
+import os
+import re
+
+import pytest
+
+from materialite_b200 import _native as nat
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "ssfft.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ssfft_\w+)\s*\(", text)))
+
+
+def test_library_is_built_and_loads():
+    assert os.path.isfile(nat.library_path()), "build with python -m materialite_b200.csrc.build"
+    nat.load_library()
+
+
+def test_every_declared_function_is_exported():
+    lib = nat.load_library()
+    names = declared_functions()
+    assert "ssfft_step" in names and "ssfft_create" in names
+    for name in names:
+        assert hasattr(lib, name), name
+    assert set(names) == set(nat.EXPORTED_SYMBOLS)
+
+
+def config(n=(16, 16, 16), precision=nat.SSFFT_MIXED, mask=(0, 1, 1, 1, 1, 1)):
+    cfg = nat.SsfftConfig()
+    for d in range(3):
+        cfg.n[d] = n[d]
+    cfg.precision = precision
+    for c in range(6):
+        cfg.stress_mask[c] = mask[c]
+    return cfg
+
+
+def estimate(cfg, evp=0, nslip=0):
+    lib = nat.load_library()
+    out = ctypes.c_size_t()
+    rc = lib.ssfft_estimate_bytes(ctypes.byref(cfg), evp, nslip, ctypes.byref(out))
+    return rc, out.value
+
+
+def test_estimate_bytes_scales_with_grid():
+    rc, small = estimate(config((32, 32, 32)))
+    assert rc == 0
+    rc, big = estimate(config((64, 64, 64)))
+    assert rc == 0 and big > 4 * small  # grid buffers dominate the fixed reduction space
+    rc, evp = estimate(config((64, 64, 64)), 1, 12)
+    assert rc == 0 and evp > big
+
+
+@pytest.mark.parametrize("n,mask,code", [((37, 8, 8), (0,) * 6, -4),      # prime factor 37
+                                         ((8, 8, 8), (0, 0.5, 0, 0, 0, 0), -1),
+                                         ((0, 8, 8), (0,) * 6, -4)])
+def test_config_validation(n, mask, code):
+    rc, _ = estimate(config(n, mask=mask))
+    assert rc == code
+    assert nat.load_library().ssfft_last_error()
+
+
+def test_invalid_precision_rejected():
+    rc, _ = estimate(config(precision=7))
+    assert rc == -1
