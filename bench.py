@@ -36,6 +36,10 @@ WORKLOADS = {
                      ltol=1e-5, precision="mixed", seed=0),
     "plain64": dict(n=64, grains=200, steps=20, dt=1.0, rate=1e-3, gtol=1e-6,
                     ltol=1e-5, precision="mixed", seed=0),
+    # Serving stream: requests with N ~ U{32,48,64,96}, 20-400 periodic Voronoi grains,
+    # elastic or FCC EVP (p = 1/2), uniaxial or biaxial strain rate 1e-3, 10-50 steps,
+    # Poisson arrivals; the first `count` requests of the seeded stream.
+    "serve": dict(count=24, rate=50.0, slots=16, seed=1000),
 }
 
 # Algorithmic HBM bytes per voxel of each Krylov-iteration kernel with float fields:
@@ -48,13 +52,12 @@ def kernel_bytes_per_voxel(n, table_mode=True):
         "yfwd": 2 * spec,                    # read + write spectrum
         "xpass": 2 * spec,
         "yinv": 2 * spec,
-        "zinv": spec + 3 * 24.0,            # read spectrum, r1, r2; write y
-        "upd1": 3 * 24.0,                   # read y, r2; write y
-        "upd2": 6 * 24.0,                   # read v, w1, w2, x; write w, x
+        "zinv": spec + 3 * 24.0,            # read spectrum, r1, r2; write y'
+        "update": 8 * 24.0,                 # read y', r2, w1, w2, x; write y'', w, x
     }
 
 
-KERNEL_NAMES = ["zfwd", "yfwd", "xpass", "yinv", "zinv", "upd1", "upd2"]
+KERNEL_NAMES = ["zfwd", "yfwd", "xpass", "yinv", "zinv", "update"]
 
 
 def cubic_mandel(C11, C12, C44):
@@ -268,17 +271,148 @@ def _ref_worker(w):
     return cpu_sample(w)
 
 
+def kernels_mode(args, w):
+    """One load increment of the workload, then ``--reps`` Krylov iterations' kernels
+    timed with CUDA events (inside the NVTX range "ssfft_profile_krylov")."""
+    rot, ids = build_microstructure(w)
+    h = make_handle(w, rot, ids, 0)
+    w1 = dict(w, steps=1)
+    run_solve(h, w1)
+    prof = h.profile_krylov(reps=args.reps)
+    h.close()
+    print(json.dumps({"workload": args.workload,
+                      "per_kernel_us": {k: prof[i] * 1e6 for i, k in enumerate(KERNEL_NAMES)},
+                      "krylov_iteration_us": prof[7] * 1e6}), flush=True)
+
+
+def serve_mode(args, w):
+    """Serving benchmark: the plain single-request FP64 GPU solve (one slot, requests one
+    after another) against the served mixed-precision stream (Poisson arrivals, up to
+    `slots` requests resident), on the same seeded requests."""
+    from materialite_b200.serving import RVEServer, latency_stats, request_stream, run_stream
+    world, rank, local = dist_setup(args.gpus)
+    count = args.count or w["count"]
+    reqs = request_stream(count, w["rate"], seed=w["seed"] + 1000 * rank)
+    voxels = sum(int(np.prod(r.dims)) for r in reqs)
+    h2d = sum(r.grain.nbytes + r.rotations.nbytes for r in reqs)
+
+    def serve(precision, slots, rate_scale):
+        for r in reqs:
+            r.keep_stress = True
+        arrivals = [r.arrival for r in reqs]
+        if rate_scale == 0:
+            for r in reqs:
+                r.arrival = 0.0
+        srv = RVEServer(device=local, max_slots=slots, precision=precision)
+        comps, span = run_stream(srv, reqs, timeout=1800)
+        launches = None
+        srv.close()
+        for r, a in zip(reqs, arrivals):
+            r.arrival = a
+        bad = [(c.tag, c.status, c.message.decode(errors="replace")) for c in comps
+               if c.status != 0]
+        if bad:
+            raise RuntimeError(f"requests failed: {bad}")
+        return comps, span, [r.stress.copy() for r in reqs]
+
+    # untimed warm-up: module load, kernel attributes, first-touch of the allocator
+    warm = request_stream(2, 0.0, seed=7)
+    srv = RVEServer(device=local, max_slots=2)
+    run_stream(srv, warm)
+    srv.close()
+    barrier(world)
+    sampler = ClockSampler(local)
+    sampler.start()
+    served, span_served, stress_mixed = serve("mixed", w["slots"], 1)
+    sat, span_sat, _ = serve("mixed", w["slots"], 0)
+    clocks = sampler.stop()
+    plain, span_plain, stress_fp64 = serve("fp64", 1, 0)
+    errs = [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(stress_mixed, stress_fp64)]
+    span_served = max_over_ranks(span_served, world, local)
+    span_sat = max_over_ranks(span_sat, world, local)
+    span_plain = max_over_ranks(span_plain, world, local)
+    total = sum_over_ranks(count, world, local)
+    lat = latency_stats(served)
+    lat_plain = latency_stats(plain)
+    value = total / span_served
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": 1, "warmup": 1, "ms_per_step": span_served * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded request stream: periodic Voronoi, uniform SO(3))",
+            "config": {"workload": f"serve: {count} requests of the serving stream at "
+                                   f"{w['rate']} req/s Poisson, N in {{32,48,64,96}}, 20-400 "
+                                   "grains, elastic or FCC EVP, uniaxial/biaxial, 10-50 steps; "
+                                   f"{w['slots']} resident slots, float fields with double "
+                                   "residuals/norms/EVP Newton",
+                       "parallelism": f"replicas x{world}", "voxels_total": voxels},
+            "served": {"solves_per_s": value, **lat, "makespan_s": span_served},
+            "saturation": {"solves_per_s": total / span_sat, "makespan_s": span_sat},
+            "plain_fp64_single_request": {"solves_per_s": total / span_plain,
+                                          **{k: v for k, v in lat_plain.items()},
+                                          "makespan_s": span_plain},
+            "served_over_plain": (total / span_served) / (total / span_plain),
+            "stress_rel_l2_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs))},
+            "clocks": clocks,
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(voxels * 48)},
+        }
+        if not args.no_roofline:
+            line["roofline"] = plain128_roofline(local)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def plain128_roofline(device):
+    """Roofline of the dominant Krylov kernel on the 128^3 plain solve (the HBM-bound
+    regime), timed live with CUDA events on the handle's stream."""
+    w = WORKLOADS["plain128"]
+    rot, ids = build_microstructure(w)
+    h = make_handle(w, rot, ids, device)
+    run_solve(h, dict(w, steps=1))
+    prof = h.profile_krylov(reps=10)
+    h.close()
+    n = w["n"]
+    V = n ** 3
+    bpv = kernel_bytes_per_voxel(n)
+    per_kernel = {k: prof[i] for i, k in enumerate(KERNEL_NAMES)}
+    dom = max(per_kernel, key=per_kernel.get)
+    peak, kind = read_peaks()
+    achieved = bpv[dom] * V / per_kernel[dom] / 1e9
+    return {"bound": "hbm", "workload": "plain128 Krylov iteration", "kernel": dom,
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "peak_kind": kind,
+            "per_kernel_us": {k: v * 1e6 for k, v in per_kernel.items()},
+            "krylov_iteration_us": prof[7] * 1e6,
+            "krylov_iteration_gbs": sum(bpv.values()) * V / prof[7] / 1e9}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="plain128", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="serve", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--mode", default="bench", choices=["bench", "kernels"],
+                    help="kernels: one load increment, then the Krylov kernels timed in "
+                         "isolation (the target of the ncu captures under profiles/)")
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--count", type=int, default=0, help="serve: number of requests")
+    ap.add_argument("--no-roofline", action="store_true")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
+    if args.mode == "kernels":
+        kernels_mode(args, w)
+        return
+    if args.workload == "serve" and args.impl == "ours":
+        serve_mode(args, w)
+        return
     if args.impl == "reference":
         reference_arm(args, w)
         return

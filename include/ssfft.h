@@ -133,6 +133,12 @@ int ssfft_set_phase_evp(ssfft_handle *h, int phase, const double stiffness[36], 
 int ssfft_set_microstructure(ssfft_handle *h, int n_orient, const double *rotations,
                              const int32_t *orient_of_point, const int32_t *phase_of_point);
 
+/* Change tolerances, iteration limits and the stress mask of an existing handle (same
+ * grid and precision).  Phases may be redefined and ssfft_set_microstructure called again
+ * on a handle: buffers are reused when large enough, so one handle can serve a sequence
+ * of solves of the same grid. */
+int ssfft_set_options(ssfft_handle *h, const ssfft_config *cfg);
+
 /* Reset the solve state to t = start (zero strain/stress, initial slip resistances). */
 int ssfft_reset(ssfft_handle *h);
 
@@ -148,6 +154,97 @@ int ssfft_commit(ssfft_handle *h, double fluctuation_scale);
 /* After a failed step: scale the carried fluctuation (1/2 on cutback,
  * small_strain_fft.py:242-244). */
 int ssfft_scale_fluctuation(ssfft_handle *h, double factor);
+
+/* Constant-rate load schedule: LoadSchedule.from_constant_rates
+ * (load_schedule.py:32-40) with the stress mask of the handle's config, and the time
+ * controls of SmallStrainFFT (small_strain_fft.py:30-51). */
+typedef struct {
+  double strain_rate[6];
+  double stress_rate[6];
+  double start_time;
+  double end_time;
+  double initial_time_increment;
+  double max_time_increment;   /* <= 0: initial_time_increment */
+  double min_time_increment;   /* <= 0: 1e-9 */
+} ssfft_rate_schedule;
+
+typedef struct {
+  int32_t status;              /* 0, or a negative SSFFT_E* code */
+  int32_t steps;               /* converged load increments */
+  int32_t cutbacks;
+  int32_t reserved;
+  int64_t newton_iterations;
+  int64_t krylov_iterations;
+  double device_seconds;       /* summed device time of the steps */
+  double mean_stress[6];
+  double mean_strain[6];
+} ssfft_solve_out;
+
+/* The whole time loop of SmallStrainFFT.run (small_strain_fft.py:106-246) for a
+ * constant-rate schedule, natively: reset, steps with cutback and dt adaptation, commits.
+ * Used by the serving loop; the Python drop-in drives ssfft_step itself. */
+int ssfft_solve_constant_rates(ssfft_handle *h, const ssfft_rate_schedule *sched,
+                               ssfft_solve_out *out);
+
+/* ---- serving ---------------------------------------------------------------------
+ * A server keeps up to max_slots RVE solves resident on one GPU, each with its own
+ * handle and CUDA stream, driven by its own host thread, so that the work of requests that
+ * arrive while others run overlaps on the device (continuous batching at request
+ * granularity).  A queued request is admitted when a slot is free and its device memory
+ * (ssfft_estimate_bytes) fits both the server's budget and cudaMemGetInfo's free memory.
+ * Results do not depend on what else runs: every reduction of a solve is private to its
+ * handle and summed in a fixed order. */
+
+/* One phase of a request (the arguments of ssfft_set_phase_elastic / _evp). */
+typedef struct {
+  int32_t kind;                /* 0: elastic, 1: crystal elasto-viscoplastic */
+  int32_t n_slip;
+  int32_t hardening;           /* SSFFT_HARDENING_* */
+  int32_t n_props;
+  double stiffness[36];
+  double schmid[SSFFT_MAX_SLIP * 6];
+  double reference_slip_rate, rate_exponent, slip_resistance, latent_ratio;
+  double hardening_props[4];
+} ssfft_phase;
+
+typedef struct {
+  ssfft_config config;         /* grid, precision, tolerances, stress mask, device ignored */
+  int32_t n_phases;
+  int32_t n_orient;
+  ssfft_phase phases[SSFFT_MAX_PHASES];
+  const double *rotations;     /* n_orient x 9, copied at submit */
+  const int32_t *orient_of_point; /* V, copied at submit */
+  const int32_t *phase_of_point;  /* V or NULL, copied at submit */
+  ssfft_rate_schedule schedule;
+  int64_t tag;                 /* caller's request id, returned in the completion */
+  double *stress_out;          /* optional host V x 6: final stress, written before the
+                                  completion is posted (caller keeps it alive) */
+} ssfft_request;
+
+typedef struct {
+  int64_t tag;
+  int32_t status;              /* 0 or a negative SSFFT_E* code */
+  int32_t slot;
+  double submit_time;          /* seconds on the server clock */
+  double start_time;           /* admitted: resources allocated, solve starts */
+  double end_time;             /* solve finished and results copied out */
+  size_t device_bytes;
+  ssfft_solve_out result;
+  char message[160];           /* ssfft_last_error() of the failing call, or "" */
+} ssfft_completion;
+
+typedef struct ssfft_server ssfft_server;
+
+int ssfft_server_create(int device, int max_slots, size_t hbm_budget_bytes,
+                        ssfft_server **out);
+int ssfft_server_submit(ssfft_server *s, const ssfft_request *req);
+/* Move up to max finished requests into out; *n_out = how many.  Non-blocking. */
+int ssfft_server_poll(ssfft_server *s, ssfft_completion *out, int max, int *n_out);
+/* Requests submitted but not yet polled (queued + running + finished-unpolled). */
+int ssfft_server_pending(ssfft_server *s);
+double ssfft_server_clock(ssfft_server *s);
+/* Stops accepting work, finishes running and queued requests, joins the threads. */
+int ssfft_server_destroy(ssfft_server *s);
 
 /* Copy a field out as float64 (V x width).  to_host = 1: dst is host memory;
  * 0: dst is device memory of the handle's device. */
@@ -193,8 +290,9 @@ int ssfft_timer(ssfft_handle *h, int start, double *seconds);
 /* Kernel timing for roofline reports: runs `reps` Krylov iterations' kernels in
  * isolation on the handle's current tangent (the MINRES buffers are overwritten) and
  * returns the mean seconds per launch of each kernel, measured with CUDA events:
- * seconds[0..4] = zfwd, yfwd, xpass, yinv, zinv(MINRES epilogue); [5] = upd1; [6] = upd2;
- * [7] = one whole Krylov iteration timed back to back.  The microstructure must be set. */
+ * seconds[0..4] = zfwd, yfwd, xpass, yinv, zinv(MINRES epilogue); [5] = the merged
+ * vector update; [6] = 0 (unused); [7] = one whole Krylov iteration timed back to back.
+ * The microstructure must be set and a solve must have run (non-uniform stress). */
 int ssfft_profile_krylov(ssfft_handle *h, int reps, double seconds[8]);
 
 #ifdef __cplusplus

@@ -38,7 +38,9 @@ EXPORTED_SYMBOLS = [
     "ssfft_reset", "ssfft_step", "ssfft_commit", "ssfft_scale_fluctuation",
     "ssfft_get_field", "ssfft_num_slip", "ssfft_apply_projection",
     "ssfft_apply_projection_device", "ssfft_stats", "ssfft_timer", "ssfft_profile_krylov",
-    "ssfft_apply_projection_noalloc",
+    "ssfft_apply_projection_noalloc", "ssfft_solve_constant_rates", "ssfft_set_options",
+    "ssfft_server_create", "ssfft_server_submit", "ssfft_server_poll", "ssfft_server_pending",
+    "ssfft_server_clock", "ssfft_server_destroy",
 ]
 
 
@@ -65,6 +67,32 @@ class SsfftStepIn(ctypes.Structure):
         ("summed_von_mises_stress", ctypes.c_double),
         ("time_step_id", ctypes.c_int32),
         ("reset_fluctuation", ctypes.c_int32),
+    ]
+
+
+class SsfftRateSchedule(ctypes.Structure):
+    _fields_ = [
+        ("strain_rate", ctypes.c_double * 6),
+        ("stress_rate", ctypes.c_double * 6),
+        ("start_time", ctypes.c_double),
+        ("end_time", ctypes.c_double),
+        ("initial_time_increment", ctypes.c_double),
+        ("max_time_increment", ctypes.c_double),
+        ("min_time_increment", ctypes.c_double),
+    ]
+
+
+class SsfftSolveOut(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32),
+        ("steps", ctypes.c_int32),
+        ("cutbacks", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("newton_iterations", ctypes.c_int64),
+        ("krylov_iterations", ctypes.c_int64),
+        ("device_seconds", ctypes.c_double),
+        ("mean_stress", ctypes.c_double * 6),
+        ("mean_strain", ctypes.c_double * 6),
     ]
 
 
@@ -126,8 +154,11 @@ def load_library():
     lib.ssfft_timer.argtypes = [P, ctypes.c_int, dp]
     lib.ssfft_profile_krylov.argtypes = [P, ctypes.c_int, dp]
     lib.ssfft_apply_projection_noalloc.argtypes = [ip, dp, P, P, P]
+    lib.ssfft_solve_constant_rates.argtypes = [P, ctypes.POINTER(SsfftRateSchedule),
+                                               ctypes.POINTER(SsfftSolveOut)]
+    lib.ssfft_set_options.argtypes = [P, ctypes.POINTER(SsfftConfig)]
     for name in EXPORTED_SYMBOLS:
-        if name != "ssfft_last_error":
+        if name not in ("ssfft_last_error", "ssfft_server_clock") and not name.startswith("ssfft_server"):
             getattr(lib, name).restype = ctypes.c_int
     _lib = lib
     return lib

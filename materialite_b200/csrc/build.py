@@ -2,8 +2,8 @@
 
     python -m materialite_b200.csrc.build
 
-Compiles ``ssfft.cu`` (which includes the kernel headers of this directory) and
-``noalloc.cu`` with nvcc into ``materialite_b200/libssfft.so``.
+Compiles ``ssfft.cu`` (which includes the kernel headers of this directory),
+``noalloc.cu`` and ``server.cu`` with nvcc into ``materialite_b200/libssfft.so``.
 """
 
 import os
@@ -32,8 +32,8 @@ def build(force=False, verbose=False):
     if (not force and os.path.isfile(out)
             and os.path.getmtime(out) >= max(os.path.getmtime(s) for s in srcs)):
         return out
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", out, os.path.join(HERE, "ssfft.cu"),
-                                   os.path.join(HERE, "noalloc.cu")]
+    cmd = [nvcc()] + NVCC_FLAGS + ["-o", out] + [os.path.join(HERE, f) for f in
+                                                 ("ssfft.cu", "noalloc.cu", "server.cu")]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

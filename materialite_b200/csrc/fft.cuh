@@ -12,10 +12,34 @@
 #define SSFFT_MAX_STAGES 16
 #define SSFFT_MAX_GENERIC_RADIX 32
 
+// Division by an invariant unsigned integer with one multiply-high, add and shift
+// (Granlund & Montgomery, "Division by invariant integers using multiplication",
+// PLDI 1994): q = (umulhi(n, m) + n) >> s with s = ceil(log2 d),
+// m = floor(2^32 (2^s - d) / d) + 1; exact for n < 2^31.
+struct FastDiv {
+  uint32_t d, m, s;
+};
+
+__host__ __device__ inline FastDiv make_fastdiv(uint32_t d) {
+  FastDiv f;
+  f.d = d;
+  uint32_t s = 0;
+  while ((1ull << s) < d) ++s;
+  f.s = s;
+  f.m = (uint32_t)(((1ull << 32) * ((1ull << s) - d)) / d + 1);
+  return f;
+}
+
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv &f) {
+  return (uint32_t)(((uint64_t)__umulhi(n, f.m) + n) >> f.s);
+}
+
 struct AxisPlan {
-  int n;                        // transform length
-  int nrad;                     // number of stages
-  int rad[SSFFT_MAX_STAGES];    // radix of each stage
+  int n;                          // transform length
+  int nrad;                       // number of stages
+  int rad[SSFFT_MAX_STAGES];      // radix of each stage
+  FastDiv mdiv[SSFFT_MAX_STAGES]; // divisor n / rad[s]
+  FastDiv nsdiv[SSFFT_MAX_STAGES];// divisor Ns = rad[0] * ... * rad[s-1]
 };
 
 // Factor n into stages: radix 8 first, then 4, 2, then odd factors (<= 32).
@@ -41,16 +65,34 @@ static inline bool make_axis_plan(int n, AxisPlan &p) {
       if (!push(f)) return false;
     }
   }
+  int ns = 1;
+  for (int st = 0; st < p.nrad; ++st) {
+    p.mdiv[st] = make_fastdiv((uint32_t)(n / p.rad[st]));
+    p.nsdiv[st] = make_fastdiv((uint32_t)ns);
+    ns *= p.rad[st];
+  }
   return true;
 }
+
+// Shared-memory index with one pad slot per 16 elements: spreads the stride-r accesses
+// of the early Stockham stages of contiguous lines over all banks.
+template <bool PAD> __device__ __forceinline__ int sidx(int i) { return PAD ? i + (i >> 4) : i; }
+__host__ __device__ inline int padded_len(int n) { return n + (n >> 4) + 1; }
 
 // Line layout in shared memory: line l starts at
 //   (l / lsub) * lstride_hi + (l % lsub) * lstride_lo
 // and its element j sits at start + j * estride.
 struct LineLayout {
   int nlines, lsub, lstride_hi, lstride_lo, estride;
+  FastDiv nl_div, lsub_div;
+  __device__ LineLayout(int nlines_, int lsub_, int hi, int lo, int es)
+      : nlines(nlines_), lsub(lsub_), lstride_hi(hi), lstride_lo(lo), estride(es) {
+    nl_div = make_fastdiv((uint32_t)nlines_);
+    lsub_div = make_fastdiv((uint32_t)lsub_);
+  }
   __device__ __forceinline__ int start(int l) const {
-    return (l / lsub) * lstride_hi + (l % lsub) * lstride_lo;
+    const int g = (int)fdiv((uint32_t)l, lsub_div);
+    return g * lstride_hi + (l - g * lsub) * lstride_lo;
   }
 };
 
@@ -113,11 +155,13 @@ __device__ __forceinline__ void bfly3(cplx<T> *v) {
   v[2] = csub<T>(m, r);
 }
 
-// One Stockham stage of radix R (R = 0: generic radix r).
-template <typename T, bool INV, bool LINES_FAST, int R>
+// One Stockham stage of radix R (R = 0: generic radix r).  PAD: shared-memory indices go
+// through sidx<true>.
+template <typename T, bool INV, bool LINES_FAST, int R, bool PAD>
 __device__ __forceinline__ void fft_stage(const cplx<T> *__restrict__ src,
                                           cplx<T> *__restrict__ dst, const LineLayout &L,
-                                          int N, int r, int Ns, const cplx<T> *tw) {
+                                          int N, int r, int Ns, const FastDiv &mdiv,
+                                          const FastDiv &nsdiv, const cplx<T> *tw) {
   const int m = N / r;
   const int total = L.nlines * m;
   const int twstep = N / (Ns * r);
@@ -125,19 +169,20 @@ __device__ __forceinline__ void fft_stage(const cplx<T> *__restrict__ src,
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
     int l, j;
     if (LINES_FAST) {
-      l = t % L.nlines;
-      j = t / L.nlines;
+      j = (int)fdiv((uint32_t)t, L.nl_div);
+      l = t - j * L.nlines;
     } else {
-      l = t / m;
-      j = t % m;
+      l = (int)fdiv((uint32_t)t, mdiv);
+      j = t - l * m;
     }
     const int base = L.start(l);
-    const int k = j % Ns;
-    const int outj = (j / Ns) * Ns * r + k;
+    const int jn = (int)fdiv((uint32_t)j, nsdiv);
+    const int k = j - jn * Ns;
+    const int outj = jn * Ns * r + k;
     if (R > 0) {
       cplx<T> v[R > 0 ? R : 1];
 #pragma unroll
-      for (int q = 0; q < R; ++q) v[q] = src[base + (j + q * m) * L.estride];
+      for (int q = 0; q < R; ++q) v[q] = src[sidx<PAD>(base + (j + q * m) * L.estride)];
       if (Ns > 1) {
 #pragma unroll
         for (int q = 1; q < R; ++q) v[q] = cmul<T>(v[q], twiddle<T, INV>(tw, q * k * twstep));
@@ -147,18 +192,18 @@ __device__ __forceinline__ void fft_stage(const cplx<T> *__restrict__ src,
       if (R == 4) bfly4<T, INV>(v);
       if (R == 8) bfly8<T, INV>(v);
 #pragma unroll
-      for (int q = 0; q < R; ++q) dst[base + (outj + q * Ns) * L.estride] = v[q];
+      for (int q = 0; q < R; ++q) dst[sidx<PAD>(base + (outj + q * Ns) * L.estride)] = v[q];
     } else {
       cplx<T> v[SSFFT_MAX_GENERIC_RADIX];
       for (int q = 0; q < r; ++q) {
-        cplx<T> a = src[base + (j + q * m) * L.estride];
+        cplx<T> a = src[sidx<PAD>(base + (j + q * m) * L.estride)];
         v[q] = (Ns > 1 && q > 0) ? cmul<T>(a, twiddle<T, INV>(tw, q * k * twstep)) : a;
       }
       for (int p = 0; p < r; ++p) {
         cplx<T> acc = v[0];
         for (int q = 1; q < r; ++q)
           acc = cadd<T>(acc, cmul<T>(v[q], twiddle<T, INV>(tw, ((p * q) % r) * rstep)));
-        dst[base + (outj + p * Ns) * L.estride] = acc;
+        dst[sidx<PAD>(base + (outj + p * Ns) * L.estride)] = acc;
       }
     }
   }
@@ -167,18 +212,20 @@ __device__ __forceinline__ void fft_stage(const cplx<T> *__restrict__ src,
 // Transform every line of `L` held in buffer `a` (scratch `b` of the same size).  The
 // caller must __syncthreads() before (data ready) and uses the returned buffer after.
 // Returns the buffer that holds the result.
-template <typename T, bool INV, bool LINES_FAST>
+template <typename T, bool INV, bool LINES_FAST, bool PAD = false>
 __device__ cplx<T> *smem_fft(cplx<T> *a, cplx<T> *b, const LineLayout &L, const AxisPlan &P,
                              const cplx<T> *tw) {
   int Ns = 1;
   for (int s = 0; s < P.nrad; ++s) {
     const int r = P.rad[s];
+    const FastDiv &md = P.mdiv[s];
+    const FastDiv &nd = P.nsdiv[s];
     switch (r) {
-      case 2: fft_stage<T, INV, LINES_FAST, 2>(a, b, L, P.n, r, Ns, tw); break;
-      case 3: fft_stage<T, INV, LINES_FAST, 3>(a, b, L, P.n, r, Ns, tw); break;
-      case 4: fft_stage<T, INV, LINES_FAST, 4>(a, b, L, P.n, r, Ns, tw); break;
-      case 8: fft_stage<T, INV, LINES_FAST, 8>(a, b, L, P.n, r, Ns, tw); break;
-      default: fft_stage<T, INV, LINES_FAST, 0>(a, b, L, P.n, r, Ns, tw); break;
+      case 2: fft_stage<T, INV, LINES_FAST, 2, PAD>(a, b, L, P.n, r, Ns, md, nd, tw); break;
+      case 3: fft_stage<T, INV, LINES_FAST, 3, PAD>(a, b, L, P.n, r, Ns, md, nd, tw); break;
+      case 4: fft_stage<T, INV, LINES_FAST, 4, PAD>(a, b, L, P.n, r, Ns, md, nd, tw); break;
+      case 8: fft_stage<T, INV, LINES_FAST, 8, PAD>(a, b, L, P.n, r, Ns, md, nd, tw); break;
+      default: fft_stage<T, INV, LINES_FAST, 0, PAD>(a, b, L, P.n, r, Ns, md, nd, tw); break;
     }
     __syncthreads();
     cplx<T> *t = a;

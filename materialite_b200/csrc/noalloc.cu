@@ -147,12 +147,12 @@ extern "C" int ssfft_apply_projection_noalloc(const int32_t n[3], const double s
   g.lz = nz >= 3 * 2048 ? 1 : std::max(1, std::min(32, 2048 / (3 * nz)));
   g.lz = (int)std::min<long long>(g.lz, (long long)nx * ny);
   g.ky = std::min(hz, 16);
-  while (g.ky > 1 && (2 * (size_t)g.ky * ny + ny) * 16 > 96 * 1024) g.ky /= 2;
+  while (g.ky > 1 && smem_y_bytes<double>(g.ky, ny) > 96 * 1024) g.ky /= 2;
   g.kx = std::min(hz, 8);
-  while (g.kx > 1 && (12 * (size_t)g.kx * nx + nx) * 16 > 100 * 1024) g.kx /= 2;
-  const size_t sz = (6 * (size_t)g.lz * nz + nz) * 16;
-  const size_t sy = (2 * (size_t)g.ky * ny + ny) * 16;
-  const size_t sx = (12 * (size_t)g.kx * nx + nx) * 16;
+  while (g.kx > 1 && smem_x_bytes<double>(g.kx, nx) > 100 * 1024) g.kx /= 2;
+  const size_t sz = smem_z_bytes<double>(g.lz, nz);
+  const size_t sy = smem_y_bytes<double>(g.ky, ny);
+  const size_t sx = smem_x_bytes<double>(g.kx, nx);
   if (sz > 200 * 1024 || sy > 200 * 1024 || sx > 200 * 1024)
     return noalloc_fail(SSFFT_E_UNSUPPORTED, "grid too large for the shared-memory FFT passes");
   ProArgs<double> pa{};

@@ -35,11 +35,28 @@ template <typename T> struct Grid {
   int kx;                          // kz columns per x-pass block
 };
 
+// Shared-memory footprint of the passes (elements of cplx<T>).  The z passes hold three
+// paired lines per (x,y) line, padded (sidx<true>); the x pass pads each component slab
+// by 64 bytes so the six slabs start on alternating bank halves.
+__host__ __device__ inline int zbuf_elems(int lz, int nz) { return padded_len(3 * lz * nz); }
+template <typename T> __host__ __device__ inline int xslab_elems(int nx, int kx) {
+  return nx * kx + 64 / (int)sizeof(cplx<T>);
+}
+template <typename T> inline size_t smem_z_bytes(int lz, int nz) {
+  return (2 * (size_t)zbuf_elems(lz, nz) + nz) * sizeof(cplx<T>);
+}
+template <typename T> inline size_t smem_y_bytes(int ky, int ny) {
+  return (2 * (size_t)ky * ny + ny) * sizeof(cplx<T>);
+}
+template <typename T> inline size_t smem_x_bytes(int kx, int nx) {
+  return (2 * 6 * (size_t)xslab_elems<T>(nx, kx) + nx) * sizeof(cplx<T>);
+}
+
 // Device-resident state of one MINRES solve (doubles; see krylov.cuh).
 struct MinresState {
   double beta1, beta, oldb, alfa, dbar, epsln, phibar, tnorm2, gmax, gmin, cs, sn;
   double delta, oldeps, gamma, phi, denom, root, anorm, ynorm, rnorm, test1, test2;
-  double s, s_prev, c_r1;
+  double s, s_prev, c_r1, coef;
   double rtol, eps;
   long long itn, maxiter;
   int istop, done;
@@ -108,8 +125,8 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
   const long long line0 = (long long)blockIdx.x * g.lz;
   const int nl = (int)min((long long)g.lz, nlines_all - line0);
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
-  cplx<T> *bufB = bufA + 3 * g.lz * nz;
-  cplx<T> *tw = bufB + 3 * g.lz * nz;
+  cplx<T> *bufB = bufA + zbuf_elems(g.lz, nz);
+  cplx<T> *tw = bufB + zbuf_elems(g.lz, nz);
   load_table<T>(tw, g.twz, nz);
   const T s = (PRO >= PRO_TANGENT_TABLE) ? (T)a.st->s : (T)1;
   for (int e = threadIdx.x; e < nl * nz; e += blockDim.x) {
@@ -118,19 +135,20 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     T tau[6];
     prologue<T, TF, PRO>(g, a, v, s, tau);
 #pragma unroll
-    for (int p = 0; p < 3; ++p) bufA[(p * nl + l) * nz + z] = mk<T>(tau[2 * p], tau[2 * p + 1]);
+    for (int p = 0; p < 3; ++p)
+      bufA[sidx<true>((p * nl + l) * nz + z)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
   }
   __syncthreads();
-  LineLayout L{3 * nl, 3 * nl, 0, nz, 1};
-  cplx<T> *res = smem_fft<T, false, false>(bufA, bufB, L, g.pz, tw);
+  const LineLayout L(3 * nl, 3 * nl, 0, nz, 1);
+  cplx<T> *res = smem_fft<T, false, false, true>(bufA, bufB, L, g.pz, tw);
   // split the paired transform: A = (Z_k + conj Z_{-k}) / 2, B = (Z_k - conj Z_{-k}) / 2i
   for (int e = threadIdx.x; e < 3 * nl * hz; e += blockDim.x) {
     const int p = e / (nl * hz);
     const int rem = e - p * nl * hz;
     const int l = rem / hz, k = rem - (rem / hz) * hz;
-    const cplx<T> Z = res[(p * nl + l) * nz + k];
+    const cplx<T> Z = res[sidx<true>((p * nl + l) * nz + k)];
     const int km = (k == 0) ? 0 : nz - k;
-    const cplx<T> Zm = res[(p * nl + l) * nz + km];
+    const cplx<T> Zm = res[sidx<true>((p * nl + l) * nz + km)];
     const cplx<T> A = mk<T>((T)0.5 * (Z.x + Zm.x), (T)0.5 * (Z.y - Zm.y));
     const cplx<T> B = mk<T>((T)0.5 * (Z.y + Zm.y), (T)0.5 * (Zm.x - Z.x));
     const long long off = (line0 + l) * hz + k;
@@ -159,7 +177,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     bufA[y * nk + kk] = base[(long long)y * hz + kk];
   }
   __syncthreads();
-  LineLayout L{nk, nk, 0, 1, nk};
+  const LineLayout L(nk, nk, 0, 1, nk);
   cplx<T> *res = smem_fft<T, INV, true>(bufA, bufB, L, g.py, tw);
   for (int e = threadIdx.x; e < ny * nk; e += blockDim.x) {
     const int y = e / nk, kk = e - (e / nk) * nk;
@@ -222,35 +240,36 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
   const int k0 = blockIdx.x * g.kx;
   const int nk = min(g.kx, hz - k0);
   const int y = blockIdx.y;
-  const int slab = nx * nk;
+  const int slab = nx * nk;                      // live elements per component
+  const int sst = xslab_elems<T>(nx, g.kx);      // padded slab stride
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
-  cplx<T> *bufB = bufA + 6 * nx * g.kx;
-  cplx<T> *tw = bufB + 6 * nx * g.kx;
+  cplx<T> *bufB = bufA + 6 * sst;
+  cplx<T> *tw = bufB + 6 * sst;
   load_table<T>(tw, g.twx, nx);
   for (int e = threadIdx.x; e < 6 * slab; e += blockDim.x) {
     const int c = e / slab, rem = e - c * slab;
     const int x = rem / nk, kk = rem - (rem / nk) * nk;
-    bufA[c * slab + x * nk + kk] = spec[c * g.S + ((long long)x * ny + y) * hz + k0 + kk];
+    bufA[c * sst + x * nk + kk] = spec[c * g.S + ((long long)x * ny + y) * hz + k0 + kk];
   }
   __syncthreads();
-  LineLayout L{6 * nk, nk, slab, 1, nk};
+  const LineLayout L(6 * nk, nk, sst, 1, nk);
   cplx<T> *res = smem_fft<T, false, true>(bufA, bufB, L, g.px, tw);
   cplx<T> *other = (res == bufA) ? bufB : bufA;
   for (int e = threadIdx.x; e < slab; e += blockDim.x) {
     const int x = e / nk, kk = e - (e / nk) * nk;
     cplx<T> m[6];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) m[c] = res[c * slab + x * nk + kk];
+    for (int c = 0; c < 6; ++c) m[c] = res[c * sst + x * nk + kk];
     green_apply<T>(g, x, y, k0 + kk, m);
 #pragma unroll
-    for (int c = 0; c < 6; ++c) res[c * slab + x * nk + kk] = m[c];
+    for (int c = 0; c < 6; ++c) res[c * sst + x * nk + kk] = m[c];
   }
   __syncthreads();
   cplx<T> *out = smem_fft<T, true, true>(res, other, L, g.px, tw);
   for (int e = threadIdx.x; e < 6 * slab; e += blockDim.x) {
     const int c = e / slab, rem = e - c * slab;
     const int x = rem / nk, kk = rem - (rem / nk) * nk;
-    spec[c * g.S + ((long long)x * ny + y) * hz + k0 + kk] = out[c * slab + x * nk + kk];
+    spec[c * g.S + ((long long)x * ny + y) * hz + k0 + kk] = out[c * sst + x * nk + kk];
   }
 }
 
@@ -266,6 +285,45 @@ template <typename T> struct EpiArgs {
   double *result;         // RESIDUAL: max |b|
 };
 
+// MINRES scalar recurrence after the matvec (Paige & Saunders 1975; scipy's minres loop
+// body up to the plane rotation).  d0 = r2 . y', d1 = y' . y', d2 = r2 . r2 where
+// y' = A v - (beta/oldb) r1 and v = r2 / beta.  The orthogonalised y'' = y' - (alfa/beta) r2
+// is formed by the next kernel; its norm follows from the three dot products:
+// |y''|^2 = d1 - 2 c d0 + c^2 d2 with c = alfa / beta.
+static __device__ __noinline__ void minres_after_matvec(MinresState *st, double d0, double d1,
+                                                 double d2) {
+  MinresState s = *st;
+  s.itn += 1;
+  s.alfa = s.s * d0;
+  s.coef = s.alfa / s.beta;
+  double beta2 = d1 - 2.0 * s.coef * d0 + s.coef * s.coef * d2;
+  if (beta2 < 0.0) beta2 = 0.0;
+  s.oldb = s.beta;
+  s.beta = sqrt(beta2);
+  s.tnorm2 += s.alfa * s.alfa + s.oldb * s.oldb + s.beta * s.beta;
+  if (s.itn == 1 && s.beta / s.beta1 <= 10.0 * s.eps) s.istop = -1;
+  s.oldeps = s.epsln;
+  s.delta = s.cs * s.dbar + s.sn * s.alfa;
+  const double gbar = s.sn * s.dbar - s.cs * s.alfa;
+  s.epsln = s.sn * s.beta;
+  s.dbar = -s.cs * s.beta;
+  s.root = hypot(gbar, s.dbar);
+  s.gamma = fmax(hypot(gbar, s.beta), s.eps);
+  s.cs = gbar / s.gamma;
+  s.sn = s.beta / s.gamma;
+  s.phi = s.cs * s.phibar;
+  s.phibar = s.sn * s.phibar;
+  s.denom = 1.0 / s.gamma;
+  s.gmax = fmax(s.gmax, s.gamma);
+  s.gmin = fmin(s.gmin, s.gamma);
+  s.s_prev = s.s;
+  s.s = (s.beta > 0.0) ? 1.0 / s.beta : 0.0;
+  s.c_r1 = (s.oldb > 0.0) ? s.beta / s.oldb : 0.0;
+  *st = s;
+}
+
+#define ZINV_PREFETCH 3  // epilogue elements per thread whose r1/r2 are loaded early
+
 template <typename T, typename TF, int EPI>
 __global__ void __launch_bounds__(SSFFT_THREADS)
     zinv_kernel(Grid<T> g, EpiArgs<TF> a, const cplx<T> *__restrict__ spec) {
@@ -277,37 +335,54 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
   const long long line0 = (long long)blockIdx.x * g.lz;
   const int nl = (int)min((long long)g.lz, nlines_all - line0);
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
-  cplx<T> *bufB = bufA + 3 * g.lz * nz;
-  cplx<T> *tw = bufB + 3 * g.lz * nz;
+  cplx<T> *bufB = bufA + zbuf_elems(g.lz, nz);
+  cplx<T> *tw = bufB + zbuf_elems(g.lz, nz);
   load_table<T>(tw, g.twz, nz);
+  const int nel = nl * nz;
+  // MINRES: issue the loads of r1 and r2 for this thread's first elements before the
+  // transform so that their latency overlaps it
+  TF p1[EPI == EPI_MINRES ? ZINV_PREFETCH : 1][6], p2[EPI == EPI_MINRES ? ZINV_PREFETCH : 1][6];
+  const bool prefetch = (EPI == EPI_MINRES) && nel <= ZINV_PREFETCH * (int)blockDim.x;
+  if (EPI == EPI_MINRES && prefetch) {
+#pragma unroll
+    for (int i = 0; i < ZINV_PREFETCH; ++i) {
+      const int e = threadIdx.x + i * blockDim.x;
+      if (e < nel) {
+        const long long v = line0 * nz + e;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          p1[i][c] = a.out[c * g.V + v];
+          p2[i][c] = a.r2[c * g.V + v];
+        }
+      }
+    }
+  }
   // rebuild the full z spectrum of Z = A + iB from the stored half (Hermitian in z)
-  for (int e = threadIdx.x; e < 3 * nl * nz; e += blockDim.x) {
-    const int p = e / (nl * nz);
-    const int rem = e - p * nl * nz;
+  for (int e = threadIdx.x; e < 3 * nel; e += blockDim.x) {
+    const int p = e / nel;
+    const int rem = e - p * nel;
     const int l = rem / nz, k = rem - (rem / nz) * nz;
     const bool low = (k < hz);
     const int ks = low ? k : nz - k;
     const long long off = (line0 + l) * hz + ks;
     const cplx<T> A = spec[(2 * p) * g.S + off];
     const cplx<T> B = spec[(2 * p + 1) * g.S + off];
-    bufA[(p * nl + l) * nz + k] = low ? mk<T>(A.x - B.y, A.y + B.x) : mk<T>(A.x + B.y, B.x - A.y);
+    bufA[sidx<true>((p * nl + l) * nz + k)] =
+        low ? mk<T>(A.x - B.y, A.y + B.x) : mk<T>(A.x + B.y, B.x - A.y);
   }
   __syncthreads();
-  LineLayout L{3 * nl, 3 * nl, 0, nz, 1};
-  cplx<T> *res = smem_fft<T, true, false>(bufA, bufB, L, g.pz, tw);
-  double acc = 0.0;
-  T s = 0, c1 = 0;
-  if (EPI == EPI_MINRES) {
-    s = (T)a.st->s;
-    c1 = (T)a.st->c_r1;
-  }
-  for (int e = threadIdx.x; e < nl * nz; e += blockDim.x) {
-    const int l = e / nz, z = e - (e / nz) * nz;
-    const long long v = (line0 + l) * nz + z;
+  const LineLayout L(3 * nl, 3 * nl, 0, nz, 1);
+  cplx<T> *res = smem_fft<T, true, false, true>(bufA, bufB, L, g.pz, tw);
+  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+  T c1 = 0;
+  if (EPI == EPI_MINRES) c1 = (T)a.st->c_r1;
+  // per-element epilogue; for MINRES r1v / r2v hold r1 and r2 at this point
+  auto finish = [&](int e, const TF *r1v, const TF *r2v) {
+    const long long v = line0 * nz + e;
     T r[6];
 #pragma unroll
     for (int p = 0; p < 3; ++p) {
-      const cplx<T> Z = res[(p * nl + l) * nz + z];
+      const cplx<T> Z = res[sidx<true>(p * nel + e)];
       r[2 * p] = Z.x;
       r[2 * p + 1] = Z.y;
     }
@@ -318,20 +393,53 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
         a.out[c * g.V + v] = (TF)r[c];
-        acc = fmax(acc, fabs((double)r[c]));
+        acc0 = fmax(acc0, fabs((double)r[c]));
       }
     } else {
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
-        const T y = r[c] - c1 * (T)a.out[c * g.V + v];
+        const T y = r[c] - c1 * (T)r1v[c];
         a.out[c * g.V + v] = (TF)y;
-        acc += (double)(s * (T)a.r2[c * g.V + v]) * (double)y;
+        acc0 += (double)r2v[c] * (double)y;
+        acc1 += (double)y * (double)y;
+        acc2 += (double)r2v[c] * (double)r2v[c];
       }
+    }
+  };
+  if (EPI == EPI_MINRES && prefetch) {
+#pragma unroll
+    for (int i = 0; i < ZINV_PREFETCH; ++i) {
+      const int e = threadIdx.x + i * blockDim.x;
+      if (e < nel) finish(e, p1[i], p2[i]);
+    }
+  } else {
+    for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+      TF q1[6], q2[6];
+      if (EPI == EPI_MINRES) {
+        const long long v = line0 * nz + e;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          q1[c] = a.out[c * g.V + v];
+          q2[c] = a.r2[c * g.V + v];
+        }
+      }
+      finish(e, q1, q2);
     }
   }
   if (EPI == EPI_STORE) return;
-  const double part = (EPI == EPI_RESIDUAL) ? block_max(acc, red) : block_sum(acc, red);
-  if (threadIdx.x == 0) a.partials[blockIdx.x] = part;
+  if (EPI == EPI_RESIDUAL) {
+    const double part = block_max(acc0, red);
+    if (threadIdx.x == 0) a.partials[blockIdx.x] = part;
+  } else {
+    const double q0 = block_sum(acc0, red);
+    const double q1 = block_sum(acc1, red);
+    const double q2 = block_sum(acc2, red);
+    if (threadIdx.x == 0) {
+      a.partials[3 * blockIdx.x] = q0;
+      a.partials[3 * blockIdx.x + 1] = q1;
+      a.partials[3 * blockIdx.x + 2] = q2;
+    }
+  }
   if (!last_block_arrives(a.ticket)) return;
   if (EPI == EPI_RESIDUAL) {
     const double m = ordered_max(a.partials, gridDim.x, 1, red);
@@ -340,10 +448,11 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
       *a.ticket = 0;
     }
   } else {
-    const double alfa = ordered_sum(a.partials, gridDim.x, 1, red);
+    const double d0 = ordered_sum(a.partials, gridDim.x, 3, red);
+    const double d1 = ordered_sum(a.partials + 1, gridDim.x, 3, red);
+    const double d2 = ordered_sum(a.partials + 2, gridDim.x, 3, red);
     if (threadIdx.x == 0) {
-      a.st->alfa = alfa;
-      a.st->itn += 1;
+      minres_after_matvec(a.st, d0, d1, d2);
       *a.ticket = 0;
     }
   }

@@ -1,0 +1,290 @@
+"""Serving many RVE homogenisation solves on one GPU (libssfft's ssfft_server_*).
+
+``RVEServer`` wraps the C server: requests (grid, phases, microstructure, constant-rate
+load schedule) are copied at submission, admitted when a slot and device memory are free,
+solved with their own handle and stream, and returned as completions carrying
+queue/start/end times.  ``request_stream`` generates the seeded request mix of the serving
+benchmark.
+"""
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _native as nat
+from .engine import hardening_props_vector
+from .microstructure import periodic_voronoi, quaternion_random_rotations
+
+
+class SsfftPhase(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32), ("n_slip", ctypes.c_int32), ("hardening", ctypes.c_int32),
+        ("n_props", ctypes.c_int32), ("stiffness", ctypes.c_double * 36),
+        ("schmid", ctypes.c_double * 72), ("reference_slip_rate", ctypes.c_double),
+        ("rate_exponent", ctypes.c_double), ("slip_resistance", ctypes.c_double),
+        ("latent_ratio", ctypes.c_double), ("hardening_props", ctypes.c_double * 4),
+    ]
+
+
+class SsfftRequest(ctypes.Structure):
+    _fields_ = [
+        ("config", nat.SsfftConfig), ("n_phases", ctypes.c_int32), ("n_orient", ctypes.c_int32),
+        ("phases", SsfftPhase * 8), ("rotations", ctypes.POINTER(ctypes.c_double)),
+        ("orient_of_point", ctypes.POINTER(ctypes.c_int32)),
+        ("phase_of_point", ctypes.POINTER(ctypes.c_int32)),
+        ("schedule", nat.SsfftRateSchedule), ("tag", ctypes.c_int64),
+        ("stress_out", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+class SsfftCompletion(ctypes.Structure):
+    _fields_ = [
+        ("tag", ctypes.c_int64), ("status", ctypes.c_int32), ("slot", ctypes.c_int32),
+        ("submit_time", ctypes.c_double), ("start_time", ctypes.c_double),
+        ("end_time", ctypes.c_double), ("device_bytes", ctypes.c_size_t),
+        ("result", nat.SsfftSolveOut), ("message", ctypes.c_char * 160),
+    ]
+
+
+def _bind(lib):
+    if getattr(lib, "_server_bound", False):
+        return lib
+    P = ctypes.c_void_p
+    lib.ssfft_server_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_size_t,
+                                        ctypes.POINTER(P)]
+    lib.ssfft_server_submit.argtypes = [P, ctypes.POINTER(SsfftRequest)]
+    lib.ssfft_server_poll.argtypes = [P, ctypes.POINTER(SsfftCompletion), ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_int)]
+    lib.ssfft_server_pending.argtypes = [P]
+    lib.ssfft_server_clock.argtypes = [P]
+    lib.ssfft_server_clock.restype = ctypes.c_double
+    lib.ssfft_server_destroy.argtypes = [P]
+    for n in ("ssfft_server_create", "ssfft_server_submit", "ssfft_server_poll",
+              "ssfft_server_pending", "ssfft_server_destroy"):
+        getattr(lib, n).restype = ctypes.c_int
+    lib._server_bound = True
+    return lib
+
+
+@dataclass
+class RVERequest:
+    """One homogenisation solve.  ``phases`` are engine.PhaseSpec objects; ``grain`` maps
+    points to rows of ``rotations``; the load is LoadSchedule.from_constant_rates with
+    ``stress_mask``."""
+    tag: int
+    dims: tuple
+    phases: list
+    rotations: np.ndarray
+    grain: np.ndarray
+    stress_mask: np.ndarray
+    strain_rate: np.ndarray
+    stress_rate: np.ndarray
+    dt: float
+    steps: int
+    phase_of_point: Optional[np.ndarray] = None
+    global_tolerance: float = 1e-6
+    linear_solver_tolerance: float = 1e-5
+    arrival: float = 0.0
+    kind: str = ""
+    keep_stress: bool = False
+    stress: Optional[np.ndarray] = field(default=None, repr=False)
+
+
+def _phase_struct(p):
+    s = SsfftPhase()
+    s.kind = 0 if p.kind == "elastic" else 1
+    C = np.asarray(p.stiffness, dtype=np.float64).ravel()
+    for i in range(36):
+        s.stiffness[i] = C[i]
+    s.latent_ratio = float(p.latent_ratio)
+    if p.kind == "evp":
+        P = np.asarray(p.schmid, dtype=np.float64).reshape(-1, 6)
+        s.n_slip = P.shape[0]
+        for i, v in enumerate(P.ravel()):
+            s.schmid[i] = v
+        s.reference_slip_rate = float(p.reference_slip_rate)
+        s.rate_exponent = float(p.rate_exponent)
+        s.slip_resistance = float(p.slip_resistance)
+        s.hardening = nat.HARDENING_IDS[p.hardening]
+        props = hardening_props_vector(p.hardening, p.hardening_props)
+        s.n_props = len(props)
+        for i, v in enumerate(props):
+            s.hardening_props[i] = v
+    return s
+
+
+class RVEServer:
+    def __init__(self, device=0, max_slots=16, hbm_budget_bytes=0, precision="mixed"):
+        self.lib = _bind(nat.load_library())
+        h = ctypes.c_void_p()
+        nat.check(self.lib.ssfft_server_create(int(device), int(max_slots),
+                                                int(hbm_budget_bytes), ctypes.byref(h)))
+        self.h = h
+        self.precision = precision
+        self._keep = {}
+
+    def clock(self):
+        return self.lib.ssfft_server_clock(self.h)
+
+    def submit(self, r: RVERequest):
+        req = SsfftRequest()
+        cfg = req.config
+        for d in range(3):
+            cfg.n[d] = int(r.dims[d])
+        cfg.precision = nat.SSFFT_FP64 if self.precision == "fp64" else nat.SSFFT_MIXED
+        cfg.max_newton_iterations = 100
+        cfg.global_tolerance = r.global_tolerance
+        cfg.strain_correction_tolerance = 1e-2
+        cfg.linear_solver_tolerance = r.linear_solver_tolerance
+        for c in range(6):
+            cfg.stress_mask[c] = float(r.stress_mask[c])
+        req.n_phases = len(r.phases)
+        for i, p in enumerate(r.phases):
+            req.phases[i] = _phase_struct(p)
+        rot = np.ascontiguousarray(r.rotations, dtype=np.float64).reshape(-1, 9)
+        grain = np.ascontiguousarray(r.grain, dtype=np.int32)
+        req.n_orient = rot.shape[0]
+        req.rotations = nat.as_double_ptr(rot)
+        req.orient_of_point = nat.as_int_ptr(grain)
+        ph = None
+        if r.phase_of_point is not None:
+            ph = np.ascontiguousarray(r.phase_of_point, dtype=np.int32)
+            req.phase_of_point = nat.as_int_ptr(ph)
+        sc = req.schedule
+        for c in range(6):
+            sc.strain_rate[c] = float(r.strain_rate[c])
+            sc.stress_rate[c] = float(r.stress_rate[c])
+        sc.start_time = 0.0
+        sc.end_time = r.dt * r.steps
+        sc.initial_time_increment = r.dt
+        req.tag = int(r.tag)
+        if r.keep_stress:
+            r.stress = np.empty((int(np.prod(r.dims)), 6))
+            req.stress_out = nat.as_double_ptr(r.stress)
+            self._keep[r.tag] = r.stress
+        nat.check(self.lib.ssfft_server_submit(self.h, ctypes.byref(req)))
+
+    def poll(self, max_items=256):
+        buf = (SsfftCompletion * max_items)()
+        n = ctypes.c_int()
+        nat.check(self.lib.ssfft_server_poll(self.h, buf, max_items, ctypes.byref(n)))
+        out = [buf[i] for i in range(n.value)]
+        for c in out:
+            self._keep.pop(c.tag, None)
+        return out
+
+    def pending(self):
+        return self.lib.ssfft_server_pending(self.h)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.ssfft_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def cubic(C11, C12, C44, scale=1.0):
+    s = np.array([1, 1, 1, np.sqrt(2), np.sqrt(2), np.sqrt(2)])
+    V = np.zeros((6, 6))
+    V[:3, :3] = C12
+    V[[0, 1, 2], [0, 1, 2]] = C11
+    V[[3, 4, 5], [3, 4, 5]] = C44
+    return V * np.outer(s, s) * scale
+
+
+def fcc_schmid():
+    from .slip_system import SlipSystem
+    return SlipSystem.octahedral().schmid_mandel()
+
+
+def elastic_phase():
+    from .engine import PhaseSpec
+    return PhaseSpec("elastic", cubic(250.0, 150.0, 120.0))
+
+
+def evp_phase(latent=1.0):
+    """FCC {111}<110>, cubic 250/150/120, reference slip rate 1e-3, n = 20, Voce with
+    tau0 = 0.1, tau_sat = 0.3 (tau_1 = 0.2), h0 = 1 (theta_1 = 0)."""
+    from .engine import PhaseSpec
+    return PhaseSpec("evp", cubic(250.0, 150.0, 120.0), fcc_schmid(), 1e-3, 20.0, 0.1, "voce",
+                     {"tau_1": 0.2, "theta_0": 1.0, "theta_1": 0.0}, latent)
+
+
+def make_request(tag, rng, sizes=(32, 48, 64, 96), grains=(20, 400), steps=(10, 50)):
+    """One request of the serving mix: grid N ~ U{sizes}, G ~ U[20, 400] periodic Voronoi
+    grains with uniform SO(3) orientations, elastic or FCC EVP with probability 1/2,
+    uniaxial or biaxial constant strain rate 1e-3, 10-50 steps (dt 1 for elastic, 0.2
+    for EVP)."""
+    n = int(rng.choice(sizes))
+    G = int(rng.integers(grains[0], grains[1] + 1))
+    ids = periodic_voronoi((n, n, n), G, rng)
+    rot = quaternion_random_rotations(G, rng)
+    is_evp = bool(rng.random() < 0.5)
+    biaxial = bool(rng.random() < 0.5)
+    nsteps = int(rng.integers(steps[0], steps[1] + 1))
+    rate = np.zeros(6)
+    mask = np.ones(6)
+    rate[0] = 1e-3
+    mask[0] = 0.0
+    if biaxial:
+        rate[1] = 1e-3
+        mask[1] = 0.0
+    return RVERequest(tag=tag, dims=(n, n, n), phases=[evp_phase() if is_evp else elastic_phase()],
+                      rotations=rot, grain=ids.astype(np.int32), stress_mask=mask,
+                      strain_rate=rate, stress_rate=np.zeros(6), dt=0.2 if is_evp else 1.0,
+                      steps=nsteps, kind=("evp" if is_evp else "elastic") + f"{n}")
+
+
+def request_stream(count, rate, seed=1000, **kw):
+    """``count`` requests with Poisson arrival times at ``rate`` per second (rate <= 0:
+    all at t = 0).  Request i draws from np.random.default_rng(seed + i)."""
+    reqs = []
+    arr_rng = np.random.default_rng(seed - 1)
+    t = 0.0
+    for i in range(count):
+        r = make_request(i, np.random.default_rng(seed + i), **kw)
+        if rate > 0:
+            t += arr_rng.exponential(1.0 / rate)
+        r.arrival = t if rate > 0 else 0.0
+        reqs.append(r)
+    return reqs
+
+
+def run_stream(server, requests, timeout=600.0, sleep=0.002):
+    """Submit each request at its arrival time (server clock) and collect completions.
+    Returns the completions in tag order and the makespan (first arrival to last end)."""
+    import time
+    t_start = server.clock()
+    pending = sorted(requests, key=lambda r: r.arrival)
+    done = {}
+    i = 0
+    deadline = time.time() + timeout
+    while len(done) < len(requests):
+        now = server.clock() - t_start
+        while i < len(pending) and pending[i].arrival <= now:
+            server.submit(pending[i])
+            i += 1
+        for c in server.poll():
+            done[c.tag] = c
+        if time.time() > deadline:
+            raise TimeoutError(f"{len(done)}/{len(requests)} requests finished in {timeout} s")
+        if i < len(pending):
+            time.sleep(min(sleep, max(0.0, pending[i].arrival - now)))
+        else:
+            time.sleep(sleep)
+    comps = [done[r.tag] for r in requests]
+    makespan = max(c.end_time for c in comps) - t_start
+    return comps, makespan
+
+
+def latency_stats(completions, requests=None):
+    lat = np.array([c.end_time - c.submit_time for c in completions])
+    return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "max_s": float(lat.max())}

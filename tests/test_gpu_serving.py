@@ -1,0 +1,84 @@
+"""Serving: requests solved concurrently on one GPU give the same result as alone, the
+native time loop equals the Python one, and admission respects the device-memory
+budget."""
+
+import numpy as np
+import pytest
+
+from materialite_b200.engine import SolverHandle, solve, unique_rotations
+from materialite_b200.serving import (RVEServer, elastic_phase, evp_phase, make_request,
+                                      run_stream)
+
+pytestmark = pytest.mark.gpu
+
+
+def small_requests():
+    rs = []
+    for tag, seed in enumerate([11, 12, 13, 14]):
+        r = make_request(tag, np.random.default_rng(seed), sizes=(32,), grains=(20, 60),
+                         steps=(4, 6))
+        r.keep_stress = True
+        rs.append(r)
+    rs[1].phases = [evp_phase()]  # one crystal-plasticity request in the mix
+    rs[1].dt = 0.2
+    return rs
+
+
+def test_result_identical_alone_and_in_the_mix():
+    reqs = small_requests()
+    alone = RVEServer(max_slots=1)
+    comps, _ = run_stream(alone, [reqs[1]])
+    alone.close()
+    assert comps[0].status == 0
+    ref = reqs[1].stress.copy()
+    reqs2 = small_requests()
+    server = RVEServer(max_slots=4)
+    comps, _ = run_stream(server, reqs2)
+    server.close()
+    assert all(c.status == 0 for c in comps)
+    # overlapping on the device did not change a single bit of the result
+    assert np.array_equal(reqs2[1].stress, ref)
+    starts = sorted(c.start_time for c in comps)
+    ends = sorted(c.end_time for c in comps)
+    assert starts[-1] < ends[0]  # all four were resident at the same time
+
+
+def test_native_time_loop_matches_python_loop():
+    r = make_request(0, np.random.default_rng(21), sizes=(32,), grains=(30, 30), steps=(5, 5))
+    r.keep_stress = True
+    server = RVEServer(max_slots=1)
+    comps, _ = run_stream(server, [r])
+    server.close()
+    assert comps[0].status == 0
+    h = SolverHandle(r.dims, r.stress_mask, "mixed", global_tolerance=r.global_tolerance,
+                     linear_solver_tolerance=r.linear_solver_tolerance)
+    h.set_phases(r.phases)
+    table, idx = unique_rotations(r.rotations[r.grain])
+    h.set_microstructure(table, idx)
+    er = r.strain_rate * (1 - r.stress_mask)
+    z = np.zeros(6)
+    out, _ = solve(h, lambda t, dt: er * dt, lambda t, dt: z, lambda t, dt: z,
+                   end_time=r.dt * r.steps, initial_time_increment=r.dt)
+    h.close()
+    # same kernels, same order of every reduction: bitwise equal
+    assert np.array_equal(out["stress"], r.stress)
+
+
+def test_admission_by_memory_budget():
+    reqs = [r for r in small_requests() if r.tag != 1][:2]
+    for r in reqs:  # two elastic requests of the same size: the same device footprint
+        r.keep_stress = False
+        r.phases = [elastic_phase()]
+        r.dt = 1.0
+    # a budget below one request's footprint: rejected, not hung
+    tiny = RVEServer(max_slots=2, hbm_budget_bytes=1 << 20)
+    comps, _ = run_stream(tiny, reqs[:1], timeout=60)
+    tiny.close()
+    assert comps[0].status == -3
+    # a budget for one request at a time: both finish, one after the other
+    one = RVEServer(max_slots=2, hbm_budget_bytes=int(1.5 * comps[0].device_bytes))
+    comps, _ = run_stream(one, reqs, timeout=120)
+    one.close()
+    assert all(c.status == 0 for c in comps)
+    a, b = sorted(comps, key=lambda c: c.start_time)
+    assert b.start_time >= a.end_time
