@@ -224,12 +224,75 @@ def cpu_sample(w, max_seconds=40.0):
     return per_solve, t_build, t_first
 
 
+SERVE_SAMPLE_STEPS = 3
+
+
+def cpu_serve_sample(seed=1000):
+    """Time the numpy oracle (this process, one core) on the first SERVE_SAMPLE_STEPS
+    load increments of a 32^3 elastic request and a 32^3 EVP request of the serving mix,
+    plus the 32^3 Gamma-hat build.  Returns seconds per increment per kind and the build
+    time."""
+    from oracle import ssfft_oracle as O
+    from materialite_b200.serving import cubic, elastic_phase, evp_phase, make_request
+    out = {}
+    t0 = time.perf_counter()
+    O.projection_operator((32, 32, 32), [0, 1, 1, 1, 1, 1])
+    out["build32"] = time.perf_counter() - t0
+    for kind in ("elastic", "evp"):
+        r = make_request(0, np.random.default_rng(seed), sizes=(32,), grains=(100, 100),
+                         steps=(10, 10))
+        if kind == "evp":
+            p = evp_phase()
+            model = O.EVPOracle(p.stiffness, p.schmid, p.reference_slip_rate, p.rate_exponent,
+                                p.slip_resistance, "voce", p.hardening_props)
+            dt = 0.2
+        else:
+            model = O.ElasticOracle(cubic(250.0, 150.0, 120.0))
+            dt = 1.0
+        load = O.LoadOracle.constant_rates(r.strain_rate, np.zeros(6), r.stress_mask)
+        t0 = time.perf_counter()
+        O.solve(r.dims, r.rotations[r.grain], model, load, end_time=SERVE_SAMPLE_STEPS * dt,
+                initial_time_increment=dt, global_tolerance=r.global_tolerance,
+                linear_solver_tolerance=r.linear_solver_tolerance)
+        out[kind] = (time.perf_counter() - t0 - out["build32"]) / SERVE_SAMPLE_STEPS
+    return out
+
+
+def cpu_serve_seconds(reqs, sample):
+    """Extrapolated oracle seconds per request: (Gamma-hat build + steps x seconds per
+    increment of its kind) x (N/32)^3."""
+    per = []
+    for r in reqs:
+        scale = (r.dims[0] / 32.0) ** 3
+        kind = "evp" if r.kind.startswith("evp") else "elastic"
+        per.append((sample["build32"] + r.steps * sample[kind]) * scale)
+    return float(np.mean(per))
+
+
+SERVE_SAMPLE_TEXT = (f"numpy oracle on the first {SERVE_SAMPLE_STEPS} load increments of a 32^3 "
+                     "elastic and a 32^3 FCC EVP request plus the 32^3 Gamma-hat build, "
+                     "extrapolated to every request of the stream by its step count and "
+                     "(N/32)^3; EVP increments after the onset of slip need more Newton "
+                     "iterations than the sampled ones, so this underestimates the CPU time")
+
+
+SINGLE_THREAD_ENV = {"OMP_NUM_THREADS": "1", "OPENBLAS_NUM_THREADS": "1",
+                     "MKL_NUM_THREADS": "1", "NUMEXPR_NUM_THREADS": "1"}
+
+
+def single_thread_pool(workers):
+    """Spawned worker processes whose BLAS/OpenMP run one thread each (the environment is
+    set before they start, so numpy picks it up)."""
+    import multiprocessing as mp
+    os.environ.update(SINGLE_THREAD_ENV)
+    return mp.get_context("spawn").Pool(workers)
+
+
 def reference_arm(args, w):
     """--impl reference: the oracle restatement of the reference's numpy path on the host
-    cores.  Each step runs one bounded sample (Gamma-hat build + first load increment)
-    per worker process, all workers in parallel; value = workers / extrapolated solve
-    time."""
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    cores (the reference is pure Python; the oracle matches it to 1e-15).  Each step runs a
+    bounded sample in every worker process at once; value = workers / extrapolated seconds
+    per solve."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -240,49 +303,51 @@ def reference_arm(args, w):
         mem_workers = max(1, int(psutil.virtual_memory().available / (12 * 2**30)))
     except Exception:
         mem_workers = 4
+    serve = args.workload == "serve"
     workers = max(1, min(cores, mem_workers, 16))
-    ctx = mp.get_context("spawn")
     times = []
-    with ctx.Pool(workers) as pool:
+    reqs = None
+    if serve:
+        from materialite_b200.serving import request_stream
+        reqs = request_stream(args.count or w["count"], w["rate"], seed=w["seed"])
+    with single_thread_pool(workers) as pool:
         for i in range(args.warmup + args.steps):
-            res = pool.map(_ref_worker, [w] * workers)
+            if serve:
+                res = pool.map(_ref_serve_worker, [w["seed"]] * workers)
+                worst = {k: max(r[k] for r in res) for k in res[0]}
+                t = cpu_serve_seconds(reqs, worst)
+            else:
+                res = pool.map(_ref_worker, [w] * workers)
+                t = max(r[0] for r in res)
             if i >= args.warmup:
-                times.append(max(r[0] for r in res))
+                times.append(t)
     per_solve = statistics.mean(times)
     value = workers / per_solve
+    if serve:
+        cfg = {"workload": f"serve: {len(reqs)} requests of the serving stream (see the ours line)"}
+        sample = SERVE_SAMPLE_TEXT
+    else:
+        cfg = {"workload": args.workload, **{k: w[k] for k in ("n", "grains", "steps")}}
+        sample = ("per worker: Gamma-hat build + first load increment, extrapolated to all "
+                  "load increments")
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_solve * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded periodic Voronoi, uniform SO(3))",
-            "impl": "reference",
-            "config": {"workload": args.workload, **{k: w[k] for k in ("n", "grains", "steps")},
-                       "l2": "inputs larger than L2"},
+            "impl": "reference", "config": cfg,
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers,
-                             "kind": "port",
-                             "sample": "per worker: Gamma-hat build + first load increment, "
-                                       "extrapolated to all load increments"},
+                             "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def _ref_worker(w):
-    os.environ.setdefault("OMP_NUM_THREADS", "1")
     return cpu_sample(w)
 
 
-def kernels_mode(args, w):
-    """One load increment of the workload, then ``--reps`` Krylov iterations' kernels
-    timed with CUDA events (inside the NVTX range "ssfft_profile_krylov")."""
-    rot, ids = build_microstructure(w)
-    h = make_handle(w, rot, ids, 0)
-    w1 = dict(w, steps=1)
-    run_solve(h, w1)
-    prof = h.profile_krylov(reps=args.reps)
-    h.close()
-    print(json.dumps({"workload": args.workload,
-                      "per_kernel_us": {k: prof[i] * 1e6 for i, k in enumerate(KERNEL_NAMES)},
-                      "krylov_iteration_us": prof[7] * 1e6}), flush=True)
+def _ref_serve_worker(seed):
+    return cpu_serve_sample(seed)
 
 
 def serve_mode(args, w):
@@ -360,10 +425,32 @@ def serve_mode(args, w):
         }
         if not args.no_roofline:
             line["roofline"] = plain128_roofline(local)
+        if world == 1 and not args.no_cpu_baseline:
+            with single_thread_pool(1) as pool:
+                sample = pool.map(_ref_serve_worker, [w["seed"]])[0]
+            per = cpu_serve_seconds(reqs, sample)
+            line["cpu_baseline"] = {"value": 1.0 / per, "unit": "solves/s", "cores": 1,
+                                    "kind": "port", "sample": SERVE_SAMPLE_TEXT}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def request_mode(args, w):
+    """One request of the serving stream (``--tag``), alone, in the chosen precision:
+    the target of per-request kernel profiles."""
+    from materialite_b200.serving import RVEServer, request_stream, run_stream
+    reqs = request_stream(args.tag + 1, 0.0, seed=w["seed"])
+    r = reqs[args.tag]
+    srv = RVEServer(max_slots=1, precision=args.precision)
+    comps, span = run_stream(srv, [r])
+    srv.close()
+    c = comps[0]
+    print(json.dumps({"tag": args.tag, "kind": r.kind, "steps": r.steps, "status": c.status,
+                      "newton": c.result.newton_iterations, "krylov": c.result.krylov_iterations,
+                      "device_s": c.result.device_seconds, "wall_s": c.end_time - c.start_time}),
+          flush=True)
 
 
 def plain128_roofline(device):
@@ -399,16 +486,21 @@ def main():
     ap.add_argument("--workload", default="serve", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--mode", default="bench", choices=["bench", "kernels"],
+    ap.add_argument("--mode", default="bench", choices=["bench", "kernels", "request"],
                     help="kernels: one load increment, then the Krylov kernels timed in "
                          "isolation (the target of the ncu captures under profiles/)")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--count", type=int, default=0, help="serve: number of requests")
     ap.add_argument("--no-roofline", action="store_true")
+    ap.add_argument("--tag", type=int, default=0, help="request mode: index in the stream")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.mode == "kernels":
         kernels_mode(args, w)
+        return
+    if args.mode == "request":
+        request_mode(args, WORKLOADS["serve"])
         return
     if args.workload == "serve" and args.impl == "ours":
         serve_mode(args, w)

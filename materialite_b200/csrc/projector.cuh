@@ -457,3 +457,157 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     }
   }
 }
+
+// ---- plane-fused passes (grids whose yz planes fit in shared memory) -------------------
+//
+// zyfwd: one block per (x plane, component pair p): tau of the pair over the whole plane
+// (prologue), real-to-complex along z, complex FFT along y, write the half spectrum of
+// both components.  yzinv is its inverse followed by the epilogue.  With xpass in between
+// a projection is three passes and the spectrum crosses HBM four times instead of eight.
+
+// Shared memory of the plane passes: two buffers of the padded plane (ny (nz + 2)
+// complex, enough for the paired z lines and for the split half spectra of two
+// components) plus the y and z twiddles.
+template <typename T> inline size_t smem_plane_bytes(int ny, int nz) {
+  return (2 * (size_t)padded_len(ny * (nz + 2)) + ny + nz) * sizeof(cplx<T>);
+}
+
+template <typename T, typename TF, int PRO>
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    zyfwd_kernel(Grid<T> g, ProArgs<TF> a, cplx<T> *__restrict__ spec) {
+  if (PRO >= PRO_TANGENT_TABLE && a.st->done) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ny = g.ny, nz = g.nz, hz = g.hz;
+  const int x = blockIdx.x, p = blockIdx.y;
+  const int cap = padded_len(ny * (nz + 2));
+  cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
+  cplx<T> *bufB = bufA + cap;
+  cplx<T> *twy = bufB + cap;
+  cplx<T> *twz = twy + ny;
+  load_table<T>(twy, g.twy, ny);
+  load_table<T>(twz, g.twz, nz);
+  const T s = (PRO >= PRO_TANGENT_TABLE) ? (T)a.st->s : (T)1;
+  const long long vbase = (long long)x * ny * nz;
+  for (int e = threadIdx.x; e < ny * nz; e += blockDim.x) {
+    T tau[6];
+    prologue<T, TF, PRO>(g, a, vbase + e, s, tau);
+    bufA[sidx<true>(e)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
+  }
+  __syncthreads();
+  const LineLayout Lz(ny, ny, 0, nz, 1);
+  cplx<T> *res = smem_fft<T, false, false, true>(bufA, bufB, Lz, g.pz, twz);
+  cplx<T> *oth = (res == bufA) ? bufB : bufA;
+  // split the paired transform into the half spectra of components 2p and 2p+1,
+  // laid out [c][y][k] for the y transform
+  const int plane = ny * hz;
+  for (int e = threadIdx.x; e < plane; e += blockDim.x) {
+    const int y = e / hz, k = e - (e / hz) * hz;
+    const cplx<T> Z = res[sidx<true>(y * nz + k)];
+    const cplx<T> Zm = res[sidx<true>(y * nz + (k == 0 ? 0 : nz - k))];
+    oth[e] = mk<T>((T)0.5 * (Z.x + Zm.x), (T)0.5 * (Z.y - Zm.y));
+    oth[plane + e] = mk<T>((T)0.5 * (Z.y + Zm.y), (T)0.5 * (Zm.x - Z.x));
+  }
+  __syncthreads();
+  const LineLayout Ly(2 * hz, hz, plane, 1, hz);
+  cplx<T> *out = smem_fft<T, false, true>(oth, res, Ly, g.py, twy);
+  for (int e = threadIdx.x; e < 2 * plane; e += blockDim.x) {
+    const int c = e / plane, rem = e - c * plane;
+    spec[(2 * p + c) * g.S + (long long)x * plane + rem] = out[e];
+  }
+}
+
+template <typename T, typename TF, int EPI>
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    yzinv_kernel(Grid<T> g, EpiArgs<TF> a, const cplx<T> *__restrict__ spec) {
+  if (EPI == EPI_MINRES && a.st->done) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[32];
+  const int ny = g.ny, nz = g.nz, hz = g.hz;
+  const int x = blockIdx.x, p = blockIdx.y;
+  const int cap = padded_len(ny * (nz + 2));
+  cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
+  cplx<T> *bufB = bufA + cap;
+  cplx<T> *twy = bufB + cap;
+  cplx<T> *twz = twy + ny;
+  load_table<T>(twy, g.twy, ny);
+  load_table<T>(twz, g.twz, nz);
+  const int plane = ny * hz;
+  for (int e = threadIdx.x; e < 2 * plane; e += blockDim.x) {
+    const int c = e / plane, rem = e - c * plane;
+    bufA[e] = spec[(2 * p + c) * g.S + (long long)x * plane + rem];
+  }
+  __syncthreads();
+  const LineLayout Ly(2 * hz, hz, plane, 1, hz);
+  cplx<T> *res = smem_fft<T, true, true>(bufA, bufB, Ly, g.py, twy);
+  cplx<T> *oth = (res == bufA) ? bufB : bufA;
+  // full z lines of Z = A + iB from the stored halves (Hermitian in z)
+  for (int e = threadIdx.x; e < ny * nz; e += blockDim.x) {
+    const int y = e / nz, k = e - (e / nz) * nz;
+    const bool low = (k < hz);
+    const int ks = low ? k : nz - k;
+    const cplx<T> A = res[y * hz + ks];
+    const cplx<T> B = res[plane + y * hz + ks];
+    oth[sidx<true>(e)] = low ? mk<T>(A.x - B.y, A.y + B.x) : mk<T>(A.x + B.y, B.x - A.y);
+  }
+  __syncthreads();
+  const LineLayout Lz(ny, ny, 0, nz, 1);
+  cplx<T> *fin = smem_fft<T, true, false, true>(oth, res, Lz, g.pz, twz);
+  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+  T c1 = 0;
+  if (EPI == EPI_MINRES) c1 = (T)a.st->c_r1;
+  const long long vbase = (long long)x * ny * nz;
+  const long long o0 = (2 * p) * g.V, o1 = (2 * p + 1) * g.V;
+  for (int e = threadIdx.x; e < ny * nz; e += blockDim.x) {
+    const long long v = vbase + e;
+    const cplx<T> Z = fin[sidx<true>(e)];
+    if (EPI == EPI_STORE) {
+      a.out[o0 + v] = (TF)Z.x;
+      a.out[o1 + v] = (TF)Z.y;
+    } else if (EPI == EPI_RESIDUAL) {
+      a.out[o0 + v] = (TF)Z.x;
+      a.out[o1 + v] = (TF)Z.y;
+      acc0 = fmax(acc0, fmax(fabs((double)Z.x), fabs((double)Z.y)));
+    } else {
+      const T y0 = Z.x - c1 * (T)a.out[o0 + v];
+      const T y1 = Z.y - c1 * (T)a.out[o1 + v];
+      const T q0 = (T)a.r2[o0 + v], q1 = (T)a.r2[o1 + v];
+      a.out[o0 + v] = (TF)y0;
+      a.out[o1 + v] = (TF)y1;
+      acc0 += (double)q0 * (double)y0 + (double)q1 * (double)y1;
+      acc1 += (double)y0 * (double)y0 + (double)y1 * (double)y1;
+      acc2 += (double)q0 * (double)q0 + (double)q1 * (double)q1;
+    }
+  }
+  if (EPI == EPI_STORE) return;
+  const int blk = blockIdx.y * gridDim.x + blockIdx.x;
+  const int nblk = gridDim.x * gridDim.y;
+  if (EPI == EPI_RESIDUAL) {
+    const double part = block_max(acc0, red);
+    if (threadIdx.x == 0) a.partials[blk] = part;
+  } else {
+    const double q0 = block_sum(acc0, red);
+    const double q1 = block_sum(acc1, red);
+    const double q2 = block_sum(acc2, red);
+    if (threadIdx.x == 0) {
+      a.partials[3 * blk] = q0;
+      a.partials[3 * blk + 1] = q1;
+      a.partials[3 * blk + 2] = q2;
+    }
+  }
+  if (!last_block_arrives(a.ticket)) return;
+  if (EPI == EPI_RESIDUAL) {
+    const double m = ordered_max(a.partials, nblk, 1, red);
+    if (threadIdx.x == 0) {
+      *a.result = m;
+      *a.ticket = 0;
+    }
+  } else {
+    const double d0 = ordered_sum(a.partials, nblk, 3, red);
+    const double d1 = ordered_sum(a.partials + 1, nblk, 3, red);
+    const double d2 = ordered_sum(a.partials + 2, nblk, 3, red);
+    if (threadIdx.x == 0) {
+      minres_after_matvec(a.st, d0, d1, d2);
+      *a.ticket = 0;
+    }
+  }
+}

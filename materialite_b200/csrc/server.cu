@@ -239,6 +239,17 @@ extern "C" int ssfft_server_create(int device, int max_slots, size_t hbm_budget_
   if (!out || max_slots < 1 || max_slots > 256)
     return ssfft_internal_fail(SSFFT_E_INVALID, "max_slots must be 1..256");
   *out = nullptr;
+  // Many slot threads each wait on their own stream; spinning waits compete for the CPU
+  // cores the other slots need to launch work.  SSFFT_SCHEDULE = spin | yield | blocking
+  // selects the waiting mode of the process's CUDA context (before it is created).
+  if (const char *sch = getenv("SSFFT_SCHEDULE")) {
+    unsigned flags = cudaDeviceScheduleAuto;
+    if (!strcmp(sch, "spin")) flags = cudaDeviceScheduleSpin;
+    if (!strcmp(sch, "yield")) flags = cudaDeviceScheduleYield;
+    if (!strcmp(sch, "blocking")) flags = cudaDeviceScheduleBlockingSync;
+    cudaSetDevice(device);
+    if (cudaSetDeviceFlags(flags) != cudaSuccess) cudaGetLastError();
+  }
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return ssfft_internal_fail(SSFFT_E_CUDA, cudaGetErrorString(e));
   size_t free_b = 0, total_b = 0;

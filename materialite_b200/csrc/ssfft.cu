@@ -113,6 +113,7 @@ struct ssfft_handle {
   int *h_cint;
   cudaGraphExec_t krylov_graph;  // one Krylov chunk, captured on first use
   bool use_graphs;
+  bool use_plane;                 // plane-fused z/y passes where they fit
   cudaEvent_t ev0, ev1, tev0, tev1;
   cudaEvent_t pev[9];
   double last_step_seconds;
@@ -200,7 +201,14 @@ template <typename T, typename TF> static int set_kernel_attrs(size_t smax) {
   CKR(smem_attr(xpass_kernel<T>, m));
   CKR(smem_attr(zinv_kernel<T, TF, EPI_STORE>, m));
   CKR(smem_attr(zinv_kernel<T, TF, EPI_RESIDUAL>, m));
+  CKR(smem_attr(zyfwd_kernel<T, TF, PRO_INPUT>, m));
+  CKR(smem_attr(zyfwd_kernel<T, TF, PRO_RESIDUAL>, m));
+  CKR(smem_attr(yzinv_kernel<T, TF, EPI_STORE>, m));
+  CKR(smem_attr(yzinv_kernel<T, TF, EPI_RESIDUAL>, m));
   if (sizeof(T) == sizeof(TF)) {
+    CKR(smem_attr(zyfwd_kernel<T, T, PRO_TANGENT_TABLE>, m));
+    CKR(smem_attr(zyfwd_kernel<T, T, PRO_TANGENT_VOXEL>, m));
+    CKR(smem_attr(yzinv_kernel<T, T, EPI_MINRES>, m));
     CKR(smem_attr(zfwd_kernel<T, T, PRO_TANGENT_TABLE>, m));
     CKR(smem_attr(zfwd_kernel<T, T, PRO_TANGENT_VOXEL>, m));
     CKR(smem_attr(zinv_kernel<T, T, EPI_MINRES>, m));
@@ -232,24 +240,56 @@ static int plan_tiles(ssfft_handle *h) {
 // ---------------------------------------------------------------------------------------
 // projector launches
 // ---------------------------------------------------------------------------------------
+// The plane-fused passes apply when a padded yz plane pair fits in shared memory.
+#define PLANE_SMEM_LIMIT (200 * 1024)
+template <typename T> static bool plane_ok(const ssfft_handle *h) {
+  return h->use_plane && smem_plane_bytes<T>(h->ny, h->nz) <= PLANE_SMEM_LIMIT;
+}
+
+// Launch the passes of one projection.  ev (optional, 6 events) is recorded before the
+// first pass and after each of the five pass slots z-fwd, y-fwd, x, y-inv, z-inv; with
+// the plane-fused passes the y slots are empty (zero time).
 template <typename T, typename TF, int PRO, int EPI>
 static int launch_projector(ssfft_handle *h, const ProArgs<TF> &pa, const EpiArgs<TF> &ea,
-                            const MinresState *st) {
+                            const MinresState *st, cudaEvent_t *ev = nullptr) {
   Grid<T> g = make_grid<T>(h);
   cplx<T> *spec = (cplx<T> *)h->spec;
-  const size_t sz = smem_z_bytes<T>(h->lz, h->nz);
-  const size_t sy = smem_y_bytes<T>(h->ky, h->ny);
+  auto rec = [&](int k) {
+    if (ev) cudaEventRecord(ev[k], h->stream);
+  };
   const size_t sx = smem_x_bytes<T>(h->kx, h->nx);
-  const int nzb = div_up((long long)h->nx * h->ny, h->lz);
-  zfwd_kernel<T, TF, PRO><<<nzb, SSFFT_THREADS, sz, h->stream>>>(g, pa, spec);
-  ypass_kernel<T, false><<<dim3(div_up(h->hz, h->ky), h->nx, 6), SSFFT_THREADS, sy,
-                           h->stream>>>(g, spec, st);
-  xpass_kernel<T><<<dim3(div_up(h->hz, h->kx), h->ny), SSFFT_THREADS, sx, h->stream>>>(
-      g, spec, st);
-  ypass_kernel<T, true><<<dim3(div_up(h->hz, h->ky), h->nx, 6), SSFFT_THREADS, sy,
-                          h->stream>>>(g, spec, st);
-  zinv_kernel<T, TF, EPI><<<nzb, SSFFT_THREADS, sz, h->stream>>>(g, ea, spec);
-  h->launches += 5;
+  rec(0);
+  if (plane_ok<T>(h)) {
+    const size_t sp = smem_plane_bytes<T>(h->ny, h->nz);
+    zyfwd_kernel<T, TF, PRO><<<dim3(h->nx, 3), SSFFT_THREADS, sp, h->stream>>>(g, pa, spec);
+    rec(1);
+    rec(2);
+    xpass_kernel<T><<<dim3(div_up(h->hz, h->kx), h->ny), SSFFT_THREADS, sx, h->stream>>>(
+        g, spec, st);
+    rec(3);
+    rec(4);
+    yzinv_kernel<T, TF, EPI><<<dim3(h->nx, 3), SSFFT_THREADS, sp, h->stream>>>(g, ea, spec);
+    rec(5);
+    h->launches += 3;
+  } else {
+    const size_t sz = smem_z_bytes<T>(h->lz, h->nz);
+    const size_t sy = smem_y_bytes<T>(h->ky, h->ny);
+    const int nzb = div_up((long long)h->nx * h->ny, h->lz);
+    zfwd_kernel<T, TF, PRO><<<nzb, SSFFT_THREADS, sz, h->stream>>>(g, pa, spec);
+    rec(1);
+    ypass_kernel<T, false><<<dim3(div_up(h->hz, h->ky), h->nx, 6), SSFFT_THREADS, sy,
+                             h->stream>>>(g, spec, st);
+    rec(2);
+    xpass_kernel<T><<<dim3(div_up(h->hz, h->kx), h->ny), SSFFT_THREADS, sx, h->stream>>>(
+        g, spec, st);
+    rec(3);
+    ypass_kernel<T, true><<<dim3(div_up(h->hz, h->ky), h->nx, 6), SSFFT_THREADS, sy,
+                            h->stream>>>(g, spec, st);
+    rec(4);
+    zinv_kernel<T, TF, EPI><<<nzb, SSFFT_THREADS, sz, h->stream>>>(g, ea, spec);
+    rec(5);
+    h->launches += 5;
+  }
   CK(cudaGetLastError());
   return 0;
 }
@@ -729,6 +769,8 @@ extern "C" int ssfft_create(const ssfft_config *cfg, ssfft_handle **out) {
   {
     const char *ng = getenv("SSFFT_NO_GRAPHS");
     h->use_graphs = !(ng && ng[0] == '1');
+    const char *np = getenv("SSFFT_NO_PLANE");
+    h->use_plane = !(np && np[0] == '1');
   }
   auto body = [&]() -> int {
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
@@ -1325,12 +1367,6 @@ template <typename T> static int profile_impl(ssfft_handle *h, int reps, double 
       (const T *)h->b, R1, R2, X, W, W2, n, h->st, 0.0, (long long)1 << 60, h->partials,
       h->tickets + TK_INIT);
   CK(cudaGetLastError());
-  Grid<T> g = make_grid<T>(h);
-  cplx<T> *spec = (cplx<T> *)h->spec;
-  const size_t sz = smem_z_bytes<T>(h->lz, h->nz);
-  const size_t sy = smem_y_bytes<T>(h->ky, h->ny);
-  const size_t sx = smem_x_bytes<T>(h->kx, h->nx);
-  const int nzb = div_up((long long)h->nx * h->ny, h->lz);
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   NvtxScope range("ssfft_profile_krylov");  // only the timed Krylov kernels
   for (int r = 0; r < reps; ++r) {
@@ -1346,45 +1382,30 @@ template <typename T> static int profile_impl(ssfft_handle *h, int reps, double 
     ea.st = h->st;
     ea.partials = h->partials;
     ea.ticket = h->tickets + TK_ZINV;
-    CK(cudaEventRecord(h->pev[0], h->stream));
     if (h->voxel_mode)
-      zfwd_kernel<T, T, PRO_TANGENT_VOXEL><<<nzb, SSFFT_THREADS, sz, h->stream>>>(g, pa, spec);
+      CKR((launch_projector<T, T, PRO_TANGENT_VOXEL, EPI_MINRES>(h, pa, ea, h->st, h->pev)));
     else
-      zfwd_kernel<T, T, PRO_TANGENT_TABLE><<<nzb, SSFFT_THREADS, sz, h->stream>>>(g, pa, spec);
-    CK(cudaEventRecord(h->pev[1], h->stream));
-    ypass_kernel<T, false><<<dim3(div_up(h->hz, h->ky), h->nx, 6), SSFFT_THREADS, sy,
-                             h->stream>>>(g, spec, h->st);
-    CK(cudaEventRecord(h->pev[2], h->stream));
-    xpass_kernel<T><<<dim3(div_up(h->hz, h->kx), h->ny), SSFFT_THREADS, sx, h->stream>>>(
-        g, spec, h->st);
-    CK(cudaEventRecord(h->pev[3], h->stream));
-    ypass_kernel<T, true><<<dim3(div_up(h->hz, h->ky), h->nx, 6), SSFFT_THREADS, sy,
-                            h->stream>>>(g, spec, h->st);
-    CK(cudaEventRecord(h->pev[4], h->stream));
-    zinv_kernel<T, T, EPI_MINRES><<<nzb, SSFFT_THREADS, sz, h->stream>>>(g, ea, spec);
-    CK(cudaEventRecord(h->pev[5], h->stream));
+      CKR((launch_projector<T, T, PRO_TANGENT_TABLE, EPI_MINRES>(h, pa, ea, h->st, h->pev)));
     CKR(launch_update<T>(h, R1, R2, W2, W, W1, X));
     CK(cudaEventRecord(h->pev[6], h->stream));
     std::swap(R1, R2);
-    CK(cudaEventRecord(h->pev[7], h->stream));
     T *old_w1 = W1;
     W1 = W2;
     W2 = W;
     W = old_w1;
     CK(cudaGetLastError());
-    CK(cudaEventSynchronize(h->pev[7]));
-    for (int k = 0; k < 7; ++k) {
+    CK(cudaEventSynchronize(h->pev[6]));
+    for (int k = 0; k < 6; ++k) {
       float ms = 0.f;
       CK(cudaEventElapsedTime(&ms, h->pev[k], h->pev[k + 1]));
       acc[k] += ms * 1e-3;
     }
     float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, h->pev[0], h->pev[7]));
+    CK(cudaEventElapsedTime(&ms, h->pev[0], h->pev[6]));
     acc[7] += ms * 1e-3;
   }
   for (int k = 0; k < 8; ++k) sec[k] = acc[k] / reps;
-  sec[6] = 0.0;  // the update is one merged kernel (seconds[5])
-  h->launches += 5LL * reps;
+  sec[6] = 0.0;
   return 0;
 }
 
