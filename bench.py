@@ -36,24 +36,40 @@ WORKLOADS = {
                      ltol=1e-5, precision="mixed", seed=0),
     "plain64": dict(n=64, grains=200, steps=20, dt=1.0, rate=1e-3, gtol=1e-6,
                     ltol=1e-5, precision="mixed", seed=0),
+    # kernel-profiling cases of the crystal-plasticity requests (per-voxel tangents)
+    "evp64": dict(n=64, grains=200, steps=5, dt=0.2, rate=1e-3, gtol=1e-6, ltol=1e-5,
+                  precision="mixed", seed=0, model="evp"),
+    "evp96": dict(n=96, grains=200, steps=5, dt=0.2, rate=1e-3, gtol=1e-6, ltol=1e-5,
+                  precision="mixed", seed=0, model="evp"),
     # Serving stream: requests with N ~ U{32,48,64,96}, 20-400 periodic Voronoi grains,
     # elastic or FCC EVP (p = 1/2), uniaxial or biaxial strain rate 1e-3, 10-50 steps,
     # Poisson arrivals; the first `count` requests of the seeded stream.
     "serve": dict(count=24, rate=50.0, slots=16, seed=1000),
 }
 
+def plane_path(n):
+    """True when the z and y passes of an n^3 float solve run plane-fused (a padded yz
+    plane pair of complex floats fits the 200 KB shared-memory budget)."""
+    padded = lambda m: m + (m >> 4) + 1
+    return (2 * padded(n * (n + 2)) + 2 * n) * 8 <= 200 * 1024
+
+
 # Algorithmic HBM bytes per voxel of each Krylov-iteration kernel with float fields:
-# planar vectors are 24 B/voxel (6 x 4 B); the half spectrum is 6 x (n/2+1)/n x 8 B.
+# planar vectors are 24 B/voxel (6 x 4 B); the half spectrum is 6 x (n/2+1)/n x 8 B.  The
+# forward z pass also applies the previous iteration's vector update (reads y', u, w1,
+# w2, x; writes u', w, x).  With the plane-fused passes the y transforms happen in shared
+# memory inside the z kernels and move no bytes of their own.
 def kernel_bytes_per_voxel(n, table_mode=True):
     spec = 6 * (n // 2 + 1) / n * 8.0
     kin = 4.0 if table_mode else 84.0
+    ypass = 0.0 if plane_path(n) else 2 * spec
     return {
-        "zfwd": 24.0 + kin + spec,          # read v, tangent; write spectrum
-        "yfwd": 2 * spec,                    # read + write spectrum
-        "xpass": 2 * spec,
-        "yinv": 2 * spec,
-        "zinv": spec + 3 * 24.0,            # read spectrum, r1, r2; write y'
-        "update": 8 * 24.0,                 # read y', r2, w1, w2, x; write y'', w, x
+        "zfwd": 8 * 24.0 + kin + spec,      # update vectors, tangent; write spectrum
+        "yfwd": ypass,
+        "xpass": 2 * spec,                  # read + write spectrum
+        "yinv": ypass,
+        "zinv": spec + 3 * 24.0,            # read spectrum, u_{j-1}, u_j; write y'
+        "update": 0.0,                      # fused into the forward z pass
     }
 
 
@@ -185,11 +201,15 @@ def sum_over_ranks(x, world, local):
 
 def make_handle(w, rot, ids, device):
     from materialite_b200.engine import PhaseSpec, SolverHandle
+    from materialite_b200.serving import evp_phase
     mask, *_ = uniaxial_x(w["rate"])
     n = w["n"]
     h = SolverHandle((n, n, n), mask, w["precision"], global_tolerance=w["gtol"],
                      linear_solver_tolerance=w["ltol"], device=device)
-    h.set_phases([PhaseSpec("elastic", cubic_mandel(250.0, 150.0, 120.0))])
+    if w.get("model") == "evp":
+        h.set_phases([evp_phase()])
+    else:
+        h.set_phases([PhaseSpec("elastic", cubic_mandel(250.0, 150.0, 120.0))])
     h.set_microstructure(rot, ids)
     return h
 
@@ -451,6 +471,27 @@ def request_mode(args, w):
                       "newton": c.result.newton_iterations, "krylov": c.result.krylov_iterations,
                       "device_s": c.result.device_seconds, "wall_s": c.end_time - c.start_time}),
           flush=True)
+
+
+def kernels_mode(args, w):
+    """One load increment of the workload, then the Krylov-iteration kernels timed with
+    CUDA events on the handle's stream (``--reps`` iterations); prints microseconds and
+    algorithmic GB/s per kernel slot."""
+    rot, ids = build_microstructure(w)
+    h = make_handle(w, rot, ids, 0)
+    run_solve(h, dict(w, steps=1))
+    prof = h.profile_krylov(reps=args.reps)
+    h.close()
+    n = w["n"]
+    V = n ** 3
+    bpv = kernel_bytes_per_voxel(n, table_mode=w.get("model") != "evp")
+    out = {"workload": args.workload, "plane_path": plane_path(n), "reps": args.reps,
+           "iteration_us": prof[7] * 1e6,
+           "iteration_gbs": sum(bpv.values()) * V / prof[7] / 1e9, "kernels": {}}
+    for i, k in enumerate(KERNEL_NAMES):
+        out["kernels"][k] = {"us": prof[i] * 1e6,
+                             "gbs": bpv[k] * V / prof[i] / 1e9 if prof[i] > 1e-7 else None}
+    print(json.dumps(out), flush=True)
 
 
 def plain128_roofline(device):

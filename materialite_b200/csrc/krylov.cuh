@@ -3,30 +3,29 @@
 // x0 = 0, no preconditioner and its default stopping tests.
 //
 // All scalars live in a MinresState in device memory and are advanced by the last
-// block of each reduction kernel, so an iteration needs no host round trip:
+// block of each reduction kernel, so an iteration needs no host round trip.  With u_j the
+// Lanczos vector of iteration j (v_j = u_j / beta_j), one iteration is three (plane-fused)
+// or five kernels:
 //
-//   zfwd(PRO_TANGENT_*)  v = s r2, tau = K v                          (projector.cuh)
+//   forward z(y)  pending update of iteration j-1: u_j = y' - (alfa/beta) u_{j-1},
+//                 w = (v_{j-1} - oldeps w1 - delta w2) / gamma, x += phi w;
+//                 last block: |x| and the stopping tests          (minres_after_update)
+//                 then tau = K (u_j / beta_j) and its forward transform
 //   ... y/x passes ...
-//   zinv(EPI_MINRES)     y' = P tau - c_r1 r1 -> r1 buffer; r2.y', y'.y', r2.r2;
-//                        last block: alfa, beta', plane rotation   (minres_after_matvec)
-//   update               y'' = y' - (alfa/beta) r2 -> r1 buffer (the next r2),
-//                        w = (v - oldeps w1 - delta w2)/gamma, x += phi w;
-//                        last block: |x| and the stopping tests    (minres_after_update)
+//   inverse z     y' = P tau - (beta_j / beta_{j-1}) u_{j-1}; u_j.y', y'.y', u_j.u_j;
+//                 last block: alfa, beta_{j+1}, plane rotation    (minres_after_matvec)
 //
-// Vectors are component-planar in the solve precision T, handled as one contiguous run of
-// 6V values; every dot product and norm accumulates in double, in a fixed order (block
-// partials summed by the last block), so results do not depend on scheduling.
+// The update needs alfa, a global dot product of the matvec, so it cannot join the
+// inverse pass; it rides on the next forward pass, which reads the same vectors anyway.
+// The last iteration's update is applied by one more forward pass, which then finds the
+// solve done.  Vectors are component-planar in the solve precision T, handled as one
+// contiguous run of 6V values; every dot product and norm accumulates in double, in a
+// fixed order (block partials summed by the last block), so results do not depend on
+// scheduling.
 #pragma once
 
 #include "common.cuh"
 #include "projector.cuh"
-
-// VW consecutive values moved as one vector access (16 bytes for float4 / double2).
-template <typename T, int VW> struct alignas(sizeof(T) * VW) Pack {
-  T v[VW];
-};
-
-template <typename T> constexpr int vec_width() { return 16 / (int)sizeof(T); }
 
 // r1 = r2 = b, x = w = w2 = 0, |b|^2; the last block initialises the MINRES state.
 template <typename T>
@@ -92,81 +91,19 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
   }
 }
 
-// Stopping tests of scipy's minres after the solution update.
-static __device__ __noinline__ void minres_after_update(MinresState *st, double x2) {
-  MinresState s = *st;
-  s.anorm = sqrt(s.tnorm2);
-  s.ynorm = sqrt(x2);
-  const double epsx = s.anorm * s.ynorm * s.eps;
-  s.rnorm = s.phibar;
-  s.test1 = (s.ynorm == 0.0 || s.anorm == 0.0) ? INFINITY : s.rnorm / (s.anorm * s.ynorm);
-  s.test2 = (s.anorm == 0.0) ? INFINITY : s.root / s.anorm;
-  const double acond = s.gmax / s.gmin;
-  if (s.istop == 0) {
-    if (1.0 + s.test2 <= 1.0) s.istop = 2;
-    if (1.0 + s.test1 <= 1.0) s.istop = 1;
-    if (s.itn >= s.maxiter) s.istop = 6;
-    if (acond >= 0.1 / s.eps) s.istop = 4;
-    if (epsx >= s.beta1) s.istop = 3;
-    if (s.test2 <= s.rtol) s.istop = 2;
-    if (s.test1 <= s.rtol) s.istop = 1;
-  }
-  if (!isfinite(s.ynorm) || !isfinite(s.beta)) s.istop = 9;  // NaN guard
-  if (s.beta == 0.0 && s.istop == 0) s.istop = 1;           // exact breakdown
-  if (s.istop != 0) s.done = 1;
-  *st = s;
-}
+// Upper bound on the default Krylov iteration limit (scipy's is 5 x ndof); the device-side
+// loop also stops there whatever limit it was given, so it can never run unbounded.
+#define KRYLOV_ITERATION_CAP 20000
 
-// y'' = y' - coef r2 (in place in y), w = (s_prev r2 - oldeps w1 - delta w2) denom into
-// wout, x += phi w, partial |x|^2.  w1 / w2 are the rotated directions (the buffers of
-// the previous w2 and w), wout the buffer of the discarded oldest one.
-template <typename T, int VW>
-__global__ void __launch_bounds__(SSFFT_THREADS)
-    minres_update_kernel(T *__restrict__ y, const T *__restrict__ r2, const T *__restrict__ w1,
-                         const T *__restrict__ w2, T *__restrict__ wout, T *__restrict__ x,
-                         long long n, MinresState *st, double *partials, unsigned int *ticket) {
-  if (st->done) return;
-  __shared__ double red[32];
-  const T coef = (T)st->coef, sv = (T)st->s_prev, oe = (T)st->oldeps, de = (T)st->delta;
-  const T dn = (T)st->denom, ph = (T)st->phi;
-  double acc = 0.0;
-  using P = Pack<T, VW>;
-  const long long nv = n / VW;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nv;
-       i += (long long)gridDim.x * blockDim.x) {
-    P yy = reinterpret_cast<const P *>(y)[i];
-    const P rr = reinterpret_cast<const P *>(r2)[i];
-    const P a1 = reinterpret_cast<const P *>(w1)[i];
-    const P a2 = reinterpret_cast<const P *>(w2)[i];
-    P xx = reinterpret_cast<const P *>(x)[i];
-    P ww;
-#pragma unroll
-    for (int k = 0; k < VW; ++k) {
-      yy.v[k] = yy.v[k] - coef * rr.v[k];
-      ww.v[k] = (sv * rr.v[k] - oe * a1.v[k] - de * a2.v[k]) * dn;
-      xx.v[k] = xx.v[k] + ph * ww.v[k];
-      acc += (double)xx.v[k] * (double)xx.v[k];
+// End of one chunk of the device-side Krylov loop (a CUDA-graph while node): run another
+// chunk unless the solve is done.  Reaching the cap ends the solve as scipy's iteration
+// limit does (istop 6, the current iterate is the answer).
+__global__ void minres_continue_kernel(MinresState *st, cudaGraphConditionalHandle cond) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    if (!st->done && st->itn > KRYLOV_ITERATION_CAP) {
+      st->istop = 6;
+      st->done = 1;
     }
-    reinterpret_cast<P *>(y)[i] = yy;
-    reinterpret_cast<P *>(wout)[i] = ww;
-    reinterpret_cast<P *>(x)[i] = xx;
-  }
-  // tail (n not a multiple of VW)
-  for (long long i = nv * VW + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    y[i] = y[i] - coef * r2[i];
-    const T wn = (sv * r2[i] - oe * w1[i] - de * w2[i]) * dn;
-    wout[i] = wn;
-    const T xi = x[i] + ph * wn;
-    x[i] = xi;
-    acc += (double)xi * (double)xi;
-  }
-  const double part = block_sum(acc, red);
-  if (threadIdx.x == 0) partials[blockIdx.x] = part;
-  if (!last_block_arrives(ticket)) return;
-  const double x2 = ordered_sum(partials, gridDim.x, 1, red);
-  if (threadIdx.x == 0) {
-    *ticket = 0;
-    minres_after_update(st, x2);
+    cudaGraphSetConditional(cond, st->done ? 0u : 1u);
   }
 }

@@ -66,13 +66,69 @@ struct MinresState {
 enum { PRO_INPUT = 0, PRO_RESIDUAL = 1, PRO_TANGENT_TABLE = 2, PRO_TANGENT_VOXEL = 3 };
 
 template <typename T> struct ProArgs {
-  const T *in;           // PRO_INPUT: tau planes; PRO_RESIDUAL: stress; TANGENT: Krylov v
+  const T *in;           // PRO_INPUT: tau planes; PRO_RESIDUAL: stress; TANGENT: Lanczos u_j
   const int32_t *gid;    // TANGENT_TABLE: tangent index per point
   const T *ktab;         // TANGENT_TABLE: [n_gid][21]
   const T *kvox;         // TANGENT_VOXEL: 21 planes of V
-  const MinresState *st; // TANGENT_*: scale 1/beta, early exit when done
+  MinresState *st;       // TANGENT_*: scalars, early exit when done
   double sbar[6];        // PRO_RESIDUAL: applied mean stress
+  // TANGENT_*: the MINRES vector update of the previous iteration, applied here
+  const T *y;            // y' of the previous iteration
+  T *unew;               // receives u_{j+1} = y' - (alfa/beta) u_j
+  const T *w1, *w2;      // the two previous search directions
+  T *wout;               // receives the new direction
+  T *x;                  // the iterate, updated in place
+  double *partials;      // per-block |x|^2
+  unsigned int *ticket;  // last-block counter of the |x|^2 reduction
 };
+
+// Stopping tests of scipy's minres after the solution update (last block of the forward
+// pass that applied it, with x2 = |x|^2).
+static __device__ __noinline__ void minres_after_update(MinresState *st, double x2) {
+  MinresState s = *st;
+  s.anorm = sqrt(s.tnorm2);
+  s.ynorm = sqrt(x2);
+  const double epsx = s.anorm * s.ynorm * s.eps;
+  s.rnorm = s.phibar;
+  s.test1 = (s.ynorm == 0.0 || s.anorm == 0.0) ? INFINITY : s.rnorm / (s.anorm * s.ynorm);
+  s.test2 = (s.anorm == 0.0) ? INFINITY : s.root / s.anorm;
+  const double acond = s.gmax / s.gmin;
+  if (s.istop == 0) {
+    if (1.0 + s.test2 <= 1.0) s.istop = 2;
+    if (1.0 + s.test1 <= 1.0) s.istop = 1;
+    if (s.itn >= s.maxiter) s.istop = 6;
+    if (acond >= 0.1 / s.eps) s.istop = 4;
+    if (epsx >= s.beta1) s.istop = 3;
+    if (s.test2 <= s.rtol) s.istop = 2;
+    if (s.test1 <= s.rtol) s.istop = 1;
+  }
+  if (!isfinite(s.ynorm) || !isfinite(s.beta)) s.istop = 9;  // NaN guard
+  if (s.beta == 0.0 && s.istop == 0) s.istop = 1;           // exact breakdown
+  if (s.istop != 0) s.done = 1;
+  *st = s;
+}
+
+// Scalars of the update pending from the previous MINRES iteration, read once per thread
+// (all iterations after the first: itn >= 1).
+template <typename T> struct PendingUpdate {
+  bool on;
+  T s, coef, sp, oe, de, dn, ph;
+};
+
+template <typename T, typename TF>
+__device__ __forceinline__ PendingUpdate<T> pending_update(const ProArgs<TF> &a) {
+  const MinresState *st = a.st;
+  PendingUpdate<T> u;
+  u.on = st->itn >= 1;
+  u.s = (T)st->s;
+  u.coef = (T)st->coef;
+  u.sp = (T)st->s_prev;
+  u.oe = (T)st->oldeps;
+  u.de = (T)st->delta;
+  u.dn = (T)st->denom;
+  u.ph = (T)st->phi;
+  return u;
+}
 
 template <typename T>
 __device__ __forceinline__ void sym6_apply(const T *k, long long kstride, const T *x,
@@ -108,6 +164,91 @@ __device__ __forceinline__ void prologue(const Grid<T> &g, const ProArgs<TF> &a,
   }
 }
 
+// Krylov prologue at one point: apply the pending update of the previous iteration
+// (u_{j+1} = y' - coef u_j, w = (v_j - oldeps w1 - delta w2) denom, x += phi w, with
+// v_j = s_prev u_j), then tau = K (s u_{j+1}).  Every block forms all six components of
+// u_{j+1} (the tangent couples them) but updates and stores only the components it owns:
+// all six (PAIR < 0) or the pair 2 PAIR, 2 PAIR + 1; |x|^2 of those accumulates into xx.
+template <typename T, typename TF, int PRO, bool ALL>
+__device__ __forceinline__ void tangent_prologue(const Grid<T> &g, const ProArgs<TF> &a,
+                                                 long long v, const PendingUpdate<T> &u,
+                                                 int pair, T *tau, double &xx) {
+  constexpr int NO = ALL ? 6 : 2;  // owned components
+  const int c0 = ALL ? 0 : 2 * pair;
+  const long long V = g.V;
+  // every load is issued before the first store: the stores may alias the loaded arrays
+  // as far as the compiler knows, and loads held back behind them would serialise
+  T r[6], yv[6], a1[NO], a2[NO], xo[NO], k[21];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) r[c] = (T)a.in[c * V + v];
+  if constexpr (PRO == PRO_TANGENT_TABLE) {
+    const TF *kp = a.ktab + (long long)a.gid[v] * 21;
+#pragma unroll
+    for (int q = 0; q < 21; ++q) k[q] = (T)kp[q];
+  } else {
+#pragma unroll
+    for (int q = 0; q < 21; ++q) k[q] = (T)a.kvox[q * V + v];
+  }
+  if (u.on) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) yv[c] = (T)a.y[c * V + v];
+#pragma unroll
+    for (int q = 0; q < NO; ++q) {
+      const long long i = (c0 + q) * V + v;
+      a1[q] = (T)a.w1[i];
+      a2[q] = (T)a.w2[i];
+      xo[q] = (T)a.x[i];
+    }
+  }
+  T vv[6];
+  if (u.on) {
+    T un[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      un[c] = yv[c] - u.coef * r[c];
+      vv[c] = u.s * un[c];
+    }
+#pragma unroll
+    for (int q = 0; q < NO; ++q) {
+      // the owned components, picked by selects (no run-time register indexing)
+      T uo, ro;
+      if constexpr (ALL) {
+        uo = un[q];
+        ro = r[q];
+      } else {
+        uo = pair == 0 ? un[q] : (pair == 1 ? un[2 + q] : un[4 + q]);
+        ro = pair == 0 ? r[q] : (pair == 1 ? r[2 + q] : r[4 + q]);
+      }
+      const long long i = (c0 + q) * V + v;
+      const T w = (u.sp * ro - u.oe * a1[q] - u.de * a2[q]) * u.dn;
+      const T xn = xo[q] + u.ph * w;
+      a.unew[i] = (TF)uo;
+      a.wout[i] = (TF)w;
+      a.x[i] = (TF)xn;
+      xx += (double)xn * (double)xn;
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) vv[c] = u.s * r[c];
+  }
+  sym6_apply<T>(k, 1, vv, tau);
+}
+
+// End of a forward pass that applied a pending update: |x|^2 over all blocks, then the
+// stopping tests in the last block to arrive.
+template <typename TF>
+__device__ __forceinline__ void finish_pending_update(const ProArgs<TF> &a, double xx, int blk,
+                                                      int nblk, double *red) {
+  const double part = block_sum(xx, red);
+  if (threadIdx.x == 0) a.partials[blk] = part;
+  if (!last_block_arrives(a.ticket)) return;
+  const double x2 = ordered_sum(a.partials, nblk, 1, red);
+  if (threadIdx.x == 0) {
+    *a.ticket = 0;
+    minres_after_update(a.st, x2);
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ void load_table(cplx<T> *dst, const cplx<T> *src, int n) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
@@ -128,12 +269,17 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
   cplx<T> *bufB = bufA + zbuf_elems(g.lz, nz);
   cplx<T> *tw = bufB + zbuf_elems(g.lz, nz);
   load_table<T>(tw, g.twz, nz);
-  const T s = (PRO >= PRO_TANGENT_TABLE) ? (T)a.st->s : (T)1;
+  PendingUpdate<T> u{};
+  if constexpr (PRO >= PRO_TANGENT_TABLE) u = pending_update<T>(a);
+  double xx = 0.0;
   for (int e = threadIdx.x; e < nl * nz; e += blockDim.x) {
     const int l = e / nz, z = e - (e / nz) * nz;
     const long long v = (line0 + l) * nz + z;
     T tau[6];
-    prologue<T, TF, PRO>(g, a, v, s, tau);
+    if constexpr (PRO >= PRO_TANGENT_TABLE)
+      tangent_prologue<T, TF, PRO, true>(g, a, v, u, 0, tau, xx);
+    else
+      prologue<T, TF, PRO>(g, a, v, (T)1, tau);
 #pragma unroll
     for (int p = 0; p < 3; ++p)
       bufA[sidx<true>((p * nl + l) * nz + z)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
@@ -154,6 +300,10 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     const long long off = (line0 + l) * hz + k;
     spec[(2 * p) * g.S + off] = A;
     spec[(2 * p + 1) * g.S + off] = B;
+  }
+  if constexpr (PRO >= PRO_TANGENT_TABLE) {
+    __shared__ double red[32];
+    if (u.on) finish_pending_update(a, xx, blockIdx.x, gridDim.x, red);
   }
 }
 
@@ -277,8 +427,9 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
 enum { EPI_STORE = 0, EPI_RESIDUAL = 1, EPI_MINRES = 2 };
 
 template <typename T> struct EpiArgs {
-  T *out;                 // STORE/RESIDUAL: output planes; MINRES: r1 (read, then y)
-  const T *r2;            // MINRES: current Lanczos vector (v = s * r2)
+  T *out;                 // STORE/RESIDUAL: output planes; MINRES: y'
+  const T *r1;            // MINRES: previous Lanczos vector u_{j-1}
+  const T *r2;            // MINRES: current Lanczos vector u_j (v = s * u_j)
   MinresState *st;        // MINRES
   double *partials;       // per-block partial results
   unsigned int *ticket;   // last-block counter
@@ -323,6 +474,7 @@ static __device__ __noinline__ void minres_after_matvec(MinresState *st, double 
 }
 
 #define ZINV_PREFETCH 3  // epilogue elements per thread whose r1/r2 are loaded early
+#define EPI_BATCH 4      // plane epilogue: elements per thread whose loads go out together
 
 template <typename T, typename TF, int EPI>
 __global__ void __launch_bounds__(SSFFT_THREADS)
@@ -351,7 +503,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
         const long long v = line0 * nz + e;
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
-          p1[i][c] = a.out[c * g.V + v];
+          p1[i][c] = a.r1[c * g.V + v];
           p2[i][c] = a.r2[c * g.V + v];
         }
       }
@@ -419,7 +571,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
         const long long v = line0 * nz + e;
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
-          q1[c] = a.out[c * g.V + v];
+          q1[c] = a.r1[c * g.V + v];
           q2[c] = a.r2[c * g.V + v];
         }
       }
@@ -472,8 +624,12 @@ template <typename T> inline size_t smem_plane_bytes(int ny, int nz) {
   return (2 * (size_t)padded_len(ny * (nz + 2)) + ny + nz) * sizeof(cplx<T>);
 }
 
-template <typename T, typename TF, int PRO>
-__global__ void __launch_bounds__(SSFFT_THREADS)
+// Plane kernels run PT threads (512 or 1024; a plane holds too few blocks per SM to
+// hide memory latency with fewer warps), at most 64 registers each.
+#define PLANE_MIN_BLOCKS(PT) ((PT) >= 1024 ? 1 : 2)
+
+template <typename T, typename TF, int PRO, int PT>
+__global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     zyfwd_kernel(Grid<T> g, ProArgs<TF> a, cplx<T> *__restrict__ spec) {
   if (PRO >= PRO_TANGENT_TABLE && a.st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -486,11 +642,16 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
   cplx<T> *twz = twy + ny;
   load_table<T>(twy, g.twy, ny);
   load_table<T>(twz, g.twz, nz);
-  const T s = (PRO >= PRO_TANGENT_TABLE) ? (T)a.st->s : (T)1;
+  PendingUpdate<T> u{};
+  if constexpr (PRO >= PRO_TANGENT_TABLE) u = pending_update<T>(a);
+  double xx = 0.0;
   const long long vbase = (long long)x * ny * nz;
   for (int e = threadIdx.x; e < ny * nz; e += blockDim.x) {
     T tau[6];
-    prologue<T, TF, PRO>(g, a, vbase + e, s, tau);
+    if constexpr (PRO >= PRO_TANGENT_TABLE)
+      tangent_prologue<T, TF, PRO, false>(g, a, vbase + e, u, p, tau, xx);
+    else
+      prologue<T, TF, PRO>(g, a, vbase + e, (T)1, tau);
     bufA[sidx<true>(e)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
   }
   __syncthreads();
@@ -514,10 +675,14 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     const int c = e / plane, rem = e - c * plane;
     spec[(2 * p + c) * g.S + (long long)x * plane + rem] = out[e];
   }
+  if constexpr (PRO >= PRO_TANGENT_TABLE) {
+    __shared__ double red[32];
+    if (u.on) finish_pending_update(a, xx, p * gridDim.x + x, gridDim.x * gridDim.y, red);
+  }
 }
 
-template <typename T, typename TF, int EPI>
-__global__ void __launch_bounds__(SSFFT_THREADS)
+template <typename T, typename TF, int EPI, int PT>
+__global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     yzinv_kernel(Grid<T> g, EpiArgs<TF> a, const cplx<T> *__restrict__ spec) {
   if (EPI == EPI_MINRES && a.st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -557,25 +722,46 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
   if (EPI == EPI_MINRES) c1 = (T)a.st->c_r1;
   const long long vbase = (long long)x * ny * nz;
   const long long o0 = (2 * p) * g.V, o1 = (2 * p + 1) * g.V;
-  for (int e = threadIdx.x; e < ny * nz; e += blockDim.x) {
-    const long long v = vbase + e;
-    const cplx<T> Z = fin[sidx<true>(e)];
-    if (EPI == EPI_STORE) {
+  if (EPI == EPI_MINRES) {
+    // batches of EPI_BATCH elements per thread: all r1 / r2 loads before the y' stores
+    constexpr int B = EPI_BATCH;
+    const int nel = ny * nz;
+    for (int e0 = threadIdx.x; e0 < nel; e0 += B * blockDim.x) {
+      T l0[B], l1[B], m0[B], m1[B];
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        const int e = e0 + b * blockDim.x;
+        if (e < nel) {
+          const long long v = vbase + e;
+          l0[b] = (T)a.r1[o0 + v];
+          l1[b] = (T)a.r1[o1 + v];
+          m0[b] = (T)a.r2[o0 + v];
+          m1[b] = (T)a.r2[o1 + v];
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        const int e = e0 + b * blockDim.x;
+        if (e < nel) {
+          const long long v = vbase + e;
+          const cplx<T> Z = fin[sidx<true>(e)];
+          const T y0 = Z.x - c1 * l0[b];
+          const T y1 = Z.y - c1 * l1[b];
+          a.out[o0 + v] = (TF)y0;
+          a.out[o1 + v] = (TF)y1;
+          acc0 += (double)m0[b] * (double)y0 + (double)m1[b] * (double)y1;
+          acc1 += (double)y0 * (double)y0 + (double)y1 * (double)y1;
+          acc2 += (double)m0[b] * (double)m0[b] + (double)m1[b] * (double)m1[b];
+        }
+      }
+    }
+  } else {
+    for (int e = threadIdx.x; e < ny * nz; e += blockDim.x) {
+      const long long v = vbase + e;
+      const cplx<T> Z = fin[sidx<true>(e)];
       a.out[o0 + v] = (TF)Z.x;
       a.out[o1 + v] = (TF)Z.y;
-    } else if (EPI == EPI_RESIDUAL) {
-      a.out[o0 + v] = (TF)Z.x;
-      a.out[o1 + v] = (TF)Z.y;
-      acc0 = fmax(acc0, fmax(fabs((double)Z.x), fabs((double)Z.y)));
-    } else {
-      const T y0 = Z.x - c1 * (T)a.out[o0 + v];
-      const T y1 = Z.y - c1 * (T)a.out[o1 + v];
-      const T q0 = (T)a.r2[o0 + v], q1 = (T)a.r2[o1 + v];
-      a.out[o0 + v] = (TF)y0;
-      a.out[o1 + v] = (TF)y1;
-      acc0 += (double)q0 * (double)y0 + (double)q1 * (double)y1;
-      acc1 += (double)y0 * (double)y0 + (double)y1 * (double)y1;
-      acc2 += (double)q0 * (double)q0 + (double)q1 * (double)q1;
+      if (EPI == EPI_RESIDUAL) acc0 = fmax(acc0, fmax(fabs((double)Z.x), fabs((double)Z.y)));
     }
   }
   if (EPI == EPI_STORE) return;

@@ -62,7 +62,7 @@ __attribute__((visibility("hidden"))) int ssfft_internal_fail(int code, const st
 // ---------------------------------------------------------------------------------------
 // handle
 // ---------------------------------------------------------------------------------------
-enum { TK_INIT = 0, TK_ZINV, TK_UPD1, TK_UPD2, TK_NORMS, TK_TSUM, TK_COUNT };
+enum { TK_INIT = 0, TK_ZINV, TK_UPD, TK_SPARE, TK_NORMS, TK_TSUM, TK_COUNT };
 #define MAX_PARTIAL_BLOCKS 65536
 
 struct ssfft_handle {
@@ -79,7 +79,7 @@ struct ssfft_handle {
   void *tw[2][3], *tn[2][3];  // [0]: float, [1]: double tables per axis
   // fields (planar, real type)
   void *eps, *sig, *sig_old, *eps_old, *dfl, *guess, *b;
-  void *kr[6];
+  void *kr[7];  // Krylov vectors: u (two), y', three directions, x
   void *spec;
   // microstructure
   bool micro_set;
@@ -114,6 +114,9 @@ struct ssfft_handle {
   cudaGraphExec_t krylov_graph;  // one Krylov chunk, captured on first use
   bool use_graphs;
   bool use_plane;                 // plane-fused z/y passes where they fit
+  cudaGraphExec_t krylov_loop;    // while node over the chunk: the whole solve on device
+  bool use_device_loop;
+  int chunk_kernels;              // kernels launched by one chunk
   cudaEvent_t ev0, ev1, tev0, tev1;
   cudaEvent_t pev[9];
   double last_step_seconds;
@@ -191,6 +194,19 @@ template <typename F> static int smem_attr(F f, int m) {
   return 0;
 }
 
+template <typename T, typename TF, int PT> static int plane_attrs(int m) {
+  CKR(smem_attr(zyfwd_kernel<T, TF, PRO_INPUT, PT>, m));
+  CKR(smem_attr(zyfwd_kernel<T, TF, PRO_RESIDUAL, PT>, m));
+  CKR(smem_attr(yzinv_kernel<T, TF, EPI_STORE, PT>, m));
+  CKR(smem_attr(yzinv_kernel<T, TF, EPI_RESIDUAL, PT>, m));
+  if (sizeof(T) == sizeof(TF)) {
+    CKR(smem_attr(zyfwd_kernel<T, T, PRO_TANGENT_TABLE, PT>, m));
+    CKR(smem_attr(zyfwd_kernel<T, T, PRO_TANGENT_VOXEL, PT>, m));
+    CKR(smem_attr(yzinv_kernel<T, T, EPI_MINRES, PT>, m));
+  }
+  return 0;
+}
+
 // Opt every shared-memory-hungry kernel instantiation into up to `smax` bytes.
 template <typename T, typename TF> static int set_kernel_attrs(size_t smax) {
   const int m = (int)smax;
@@ -201,14 +217,9 @@ template <typename T, typename TF> static int set_kernel_attrs(size_t smax) {
   CKR(smem_attr(xpass_kernel<T>, m));
   CKR(smem_attr(zinv_kernel<T, TF, EPI_STORE>, m));
   CKR(smem_attr(zinv_kernel<T, TF, EPI_RESIDUAL>, m));
-  CKR(smem_attr(zyfwd_kernel<T, TF, PRO_INPUT>, m));
-  CKR(smem_attr(zyfwd_kernel<T, TF, PRO_RESIDUAL>, m));
-  CKR(smem_attr(yzinv_kernel<T, TF, EPI_STORE>, m));
-  CKR(smem_attr(yzinv_kernel<T, TF, EPI_RESIDUAL>, m));
+  CKR((plane_attrs<T, TF, 512>(m)));
+  CKR((plane_attrs<T, TF, 1024>(m)));
   if (sizeof(T) == sizeof(TF)) {
-    CKR(smem_attr(zyfwd_kernel<T, T, PRO_TANGENT_TABLE>, m));
-    CKR(smem_attr(zyfwd_kernel<T, T, PRO_TANGENT_VOXEL>, m));
-    CKR(smem_attr(yzinv_kernel<T, T, EPI_MINRES>, m));
     CKR(smem_attr(zfwd_kernel<T, T, PRO_TANGENT_TABLE>, m));
     CKR(smem_attr(zfwd_kernel<T, T, PRO_TANGENT_VOXEL>, m));
     CKR(smem_attr(zinv_kernel<T, T, EPI_MINRES>, m));
@@ -246,6 +257,12 @@ template <typename T> static bool plane_ok(const ssfft_handle *h) {
   return h->use_plane && smem_plane_bytes<T>(h->ny, h->nz) <= PLANE_SMEM_LIMIT;
 }
 
+// Threads of a plane block: 1024 when a single block fits an SM (228 KB of shared memory),
+// else 512.
+template <typename T> static int plane_threads(const ssfft_handle *h) {
+  return smem_plane_bytes<T>(h->ny, h->nz) > 113 * 1024 ? 1024 : 512;
+}
+
 // Launch the passes of one projection.  ev (optional, 6 events) is recorded before the
 // first pass and after each of the five pass slots z-fwd, y-fwd, x, y-inv, z-inv; with
 // the plane-fused passes the y slots are empty (zero time).
@@ -261,14 +278,21 @@ static int launch_projector(ssfft_handle *h, const ProArgs<TF> &pa, const EpiArg
   rec(0);
   if (plane_ok<T>(h)) {
     const size_t sp = smem_plane_bytes<T>(h->ny, h->nz);
-    zyfwd_kernel<T, TF, PRO><<<dim3(h->nx, 3), SSFFT_THREADS, sp, h->stream>>>(g, pa, spec);
+    const int pt = plane_threads<T>(h);
+    if (pt == 1024)
+      zyfwd_kernel<T, TF, PRO, 1024><<<dim3(h->nx, 3), 1024, sp, h->stream>>>(g, pa, spec);
+    else
+      zyfwd_kernel<T, TF, PRO, 512><<<dim3(h->nx, 3), 512, sp, h->stream>>>(g, pa, spec);
     rec(1);
     rec(2);
     xpass_kernel<T><<<dim3(div_up(h->hz, h->kx), h->ny), SSFFT_THREADS, sx, h->stream>>>(
         g, spec, st);
     rec(3);
     rec(4);
-    yzinv_kernel<T, TF, EPI><<<dim3(h->nx, 3), SSFFT_THREADS, sp, h->stream>>>(g, ea, spec);
+    if (pt == 1024)
+      yzinv_kernel<T, TF, EPI, 1024><<<dim3(h->nx, 3), 1024, sp, h->stream>>>(g, ea, spec);
+    else
+      yzinv_kernel<T, TF, EPI, 512><<<dim3(h->nx, 3), 512, sp, h->stream>>>(g, ea, spec);
     rec(5);
     h->launches += 3;
   } else {
@@ -333,77 +357,169 @@ template <typename T> static int reproject(ssfft_handle *h, T *x) {
 // ---------------------------------------------------------------------------------------
 // MINRES driver
 // ---------------------------------------------------------------------------------------
-// The merged MINRES vector update (krylov.cuh), 16-byte vector accesses when the 6V values
-// allow it.
+// Krylov vectors of one solve (krylov.cuh).  At the start of iteration j, P holds u_{j-1},
+// Q holds u_{j-2} (dead) and receives u_j from the forward pass, Y holds y' of iteration
+// j-1; W1 and W2 are the two previous directions and W receives the new one.  After the
+// iteration P and Q swap and the directions rotate (periods 2 and 3).  minres_init_kernel
+// writes b into both P and Q, so the first iteration (no pending update) reads u_1 = b
+// from either.
+template <typename T> struct KrylovBufs {
+  T *P, *Q, *Y, *W, *W1, *W2, *X;
+  void advance() {
+    std::swap(P, Q);
+    T *old_w1 = W1;
+    W1 = W2;
+    W2 = W;
+    W = old_w1;
+  }
+};
+
+template <typename T> static KrylovBufs<T> krylov_bufs(ssfft_handle *h) {
+  KrylovBufs<T> k;
+  k.P = (T *)h->kr[0];
+  k.Q = (T *)h->kr[1];
+  k.W = (T *)h->kr[2];
+  k.W1 = (T *)h->kr[3];
+  k.W2 = (T *)h->kr[4];
+  k.X = (T *)h->kr[5];
+  k.Y = (T *)h->kr[6];
+  return k;
+}
+
+// r1 = r2 = b, x = w = w2 = 0 (in the names of the first iteration) and the MINRES state.
 template <typename T>
-static int launch_update(ssfft_handle *h, T *y, const T *r2, const T *w1, const T *w2, T *wout,
-                         T *x) {
-  const long long n = 6 * h->V;
-  constexpr int VW = vec_width<T>();
-  const int blocks =
-      std::max(1, std::min(div_up(n / VW + 1, SSFFT_THREADS), MAX_PARTIAL_BLOCKS / 16));
-  minres_update_kernel<T, VW><<<blocks, SSFFT_THREADS, 0, h->stream>>>(
-      y, r2, w1, w2, wout, x, n, h->st, h->partials, h->tickets + TK_UPD2);
+static int launch_minres_init(ssfft_handle *h, const KrylovBufs<T> &k, double rtol,
+                              long long maxiter) {
+  minres_init_kernel<T><<<h->red_blocks, SSFFT_THREADS, 0, h->stream>>>(
+      (const T *)h->b, k.P, k.Q, k.X, k.W, k.W2, 6 * h->V, h->st, rtol, maxiter, h->partials,
+      h->tickets + TK_INIT);
   h->launches += 1;
   CK(cudaGetLastError());
   return 0;
 }
 
+// One MINRES iteration: the projector passes with the pending vector update in the
+// forward prologue and the scalar recurrence in the inverse epilogue.  ev as in
+// launch_projector.
+template <typename T>
+static int krylov_iteration(ssfft_handle *h, const KrylovBufs<T> &k, cudaEvent_t *ev = nullptr) {
+  ProArgs<T> pa{};
+  pa.in = k.P;
+  pa.gid = h->gid;
+  pa.ktab = (const T *)h->ktab;
+  pa.kvox = (const T *)h->kvox;
+  pa.st = h->st;
+  pa.y = k.Y;
+  pa.unew = k.Q;
+  pa.w1 = k.W1;
+  pa.w2 = k.W2;
+  pa.wout = k.W;
+  pa.x = k.X;
+  pa.partials = h->partials;
+  pa.ticket = h->tickets + TK_UPD;
+  EpiArgs<T> ea{};
+  ea.out = k.Y;
+  ea.r1 = k.P;
+  ea.r2 = k.Q;
+  ea.st = h->st;
+  ea.partials = h->partials;
+  ea.ticket = h->tickets + TK_ZINV;
+  if (h->voxel_mode)
+    return launch_projector<T, T, PRO_TANGENT_VOXEL, EPI_MINRES>(h, pa, ea, h->st, ev);
+  return launch_projector<T, T, PRO_TANGENT_TABLE, EPI_MINRES>(h, pa, ea, h->st, ev);
+}
+
 #define KRYLOV_CHUNK 6  // a multiple of both buffer-rotation periods (2 and 3)
 #define MIXED_RTOL_FLOOR 1.0e-6
+
+template <typename T>
+static int finish_minres(ssfft_handle *h, long long *iters, T **xout, T *X) {
+  if (h->h_st->istop == 9) return fail(SSFFT_E_NAN, "non-finite value in the Krylov solve");
+  *iters = h->h_st->itn;
+  *xout = X;
+  return 0;
+}
 
 template <typename T> static int run_minres(ssfft_handle *h, long long *iters, T **xout) {
   NvtxScope range("ssfft_minres");
   const long long n = 6 * h->V;
-  T *R1 = (T *)h->kr[0], *R2 = (T *)h->kr[1], *W = (T *)h->kr[2], *W1 = (T *)h->kr[3],
-    *W2 = (T *)h->kr[4], *X = (T *)h->kr[5];
-  const long long maxiter =
-      h->cfg.max_krylov_iterations > 0 ? h->cfg.max_krylov_iterations : 5 * n;
+  const KrylovBufs<T> k0 = krylov_bufs<T>(h);
+  // scipy's default limit is 5 x ndof; past KRYLOV_ITERATION_CAP a solve is not going to
+  // converge in any useful time, so every limit is clamped there (the device-side loop
+  // must end by itself)
+  const long long maxiter = std::min<long long>(
+      h->cfg.max_krylov_iterations > 0 ? h->cfg.max_krylov_iterations : 5 * n,
+      KRYLOV_ITERATION_CAP);
   // float Krylov vectors cannot resolve relative residuals much below 1e-6
   const double rtol = h->fp64 ? h->cfg.linear_solver_tolerance
                               : std::max(h->cfg.linear_solver_tolerance, MIXED_RTOL_FLOOR);
-  minres_init_kernel<T><<<h->red_blocks, SSFFT_THREADS, 0, h->stream>>>(
-      (const T *)h->b, R1, R2, X, W, W2, n, h->st, rtol, maxiter,
-      h->partials, h->tickets + TK_INIT);
-  h->launches += 1;
-  CK(cudaGetLastError());
-  // One chunk of KRYLOV_CHUNK iterations.  The buffer roles rotate with periods 2 (r1/r2)
-  // and 3 (w, w1, w2); a chunk of 6 leaves them where they started, so the same launch
-  // sequence (and a CUDA graph captured from it) repeats until the solve is done.  Kernels
-  // return at once when the device state says done.
+  CKR(launch_minres_init<T>(h, k0, rtol, maxiter));
+  T *X = k0.X;
+  // One chunk of KRYLOV_CHUNK iterations.  A chunk of 6 leaves the buffer roles where they
+  // started, so the same launch sequence (and a CUDA graph captured from it) repeats until
+  // the solve is done.  Kernels return at once when the device state says done.
   auto chunk = [&]() -> int {
-    T *r1 = R1, *r2 = R2, *w = W, *w1 = W1, *w2 = W2;
+    KrylovBufs<T> k = k0;
     for (int i = 0; i < KRYLOV_CHUNK; ++i) {
-      ProArgs<T> pa{};
-      pa.in = r2;
-      pa.gid = h->gid;
-      pa.ktab = (const T *)h->ktab;
-      pa.kvox = (const T *)h->kvox;
-      pa.st = h->st;
-      EpiArgs<T> ea{};
-      ea.out = r1;
-      ea.r2 = r2;
-      ea.st = h->st;
-      ea.partials = h->partials;
-      ea.ticket = h->tickets + TK_ZINV;
-      if (h->voxel_mode)
-        CKR((launch_projector<T, T, PRO_TANGENT_VOXEL, EPI_MINRES>(h, pa, ea, h->st)));
-      else
-        CKR((launch_projector<T, T, PRO_TANGENT_TABLE, EPI_MINRES>(h, pa, ea, h->st)));
-      CKR(launch_update<T>(h, r1, r2, w2, w, w1, X));
-      std::swap(r1, r2);
-      T *old_w1 = w1;
-      w1 = w2;
-      w2 = w;
-      w = old_w1;
+      CKR(krylov_iteration<T>(h, k));
+      k.advance();
     }
     return 0;
   };
+  if (h->use_device_loop) {
+    // the whole Krylov loop on the device: a while node whose body is one chunk followed
+    // by minres_continue_kernel, which sets the loop condition from the MINRES state
+    if (!h->krylov_loop) {
+      const long long launches_before = h->launches;
+      cudaGraph_t graph = nullptr;
+      CK(cudaGraphCreate(&graph, 0));
+      cudaGraphConditionalHandle cond;
+      cudaError_t e = cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault);
+      cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+      np.conditional.handle = cond;
+      np.conditional.type = cudaGraphCondTypeWhile;
+      np.conditional.size = 1;
+      cudaGraphNode_t node;
+      if (e == cudaSuccess) e = cudaGraphAddNode(&node, graph, nullptr, 0, &np);
+      cudaGraph_t body = (e == cudaSuccess) ? np.conditional.phGraph_out[0] : nullptr;
+      if (e == cudaSuccess)
+        e = cudaStreamBeginCaptureToGraph(h->stream, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return fail(SSFFT_E_CUDA, std::string("device loop setup: ") + cudaGetErrorString(e));
+      }
+      const int rc = chunk();
+      minres_continue_kernel<<<1, 32, 0, h->stream>>>(h->st, cond);
+      cudaGraph_t captured = nullptr;
+      e = cudaStreamEndCapture(h->stream, &captured);
+      h->chunk_kernels = (int)(h->launches - launches_before);
+      h->launches = launches_before;
+      if (rc || e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        if (rc) return rc;
+        return fail(SSFFT_E_CUDA, std::string("device loop capture: ") + cudaGetErrorString(e));
+      }
+      e = cudaGraphInstantiate(&h->krylov_loop, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) {
+        h->krylov_loop = nullptr;
+        return fail(SSFFT_E_CUDA, std::string("device loop instantiate: ") + cudaGetErrorString(e));
+      }
+    }
+    CK(cudaGraphLaunch(h->krylov_loop, h->stream));
+    CK(cudaMemcpyAsync(h->h_st, h->st, sizeof(MinresState), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const long long chunks = (h->h_st->itn + KRYLOV_CHUNK - 1) / KRYLOV_CHUNK;
+    h->launches += std::max(1LL, chunks) * (h->chunk_kernels + 1);
+    return finish_minres(h, iters, xout, X);
+  }
   if (h->use_graphs && !h->krylov_graph) {
     cudaGraph_t graph = nullptr;
     const long long launches_before = h->launches;  // capture records, it does not launch
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     const int rc = chunk();
+    h->chunk_kernels = (int)(h->launches - launches_before);
     h->launches = launches_before;
     cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
     if (rc) {
@@ -423,7 +539,7 @@ template <typename T> static int run_minres(ssfft_handle *h, long long *iters, T
     for (int c = 0; c < (round == 0 ? 2 : 1); ++c) {
       if (h->krylov_graph) {
         CK(cudaGraphLaunch(h->krylov_graph, h->stream));
-        h->launches += 6LL * KRYLOV_CHUNK;
+        h->launches += h->chunk_kernels;
       } else {
         CKR(chunk());
       }
@@ -433,10 +549,7 @@ template <typename T> static int run_minres(ssfft_handle *h, long long *iters, T
     CK(cudaStreamSynchronize(h->stream));
     if (h->h_st->done) break;
   }
-  if (h->h_st->istop == 9) return fail(SSFFT_E_NAN, "non-finite value in the Krylov solve");
-  *iters = h->h_st->itn;
-  *xout = X;
-  return 0;
+  return finish_minres(h, iters, xout, X);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -681,7 +794,7 @@ static void free_handle(ssfft_handle *h) {
     }
   void *ptrs[] = {h->eps, h->sig,
                   h->sig_old, h->eps_old, h->dfl, h->guess, h->b, h->kr[0], h->kr[1],
-                  h->kr[2], h->kr[3], h->kr[4], h->kr[5], h->spec, h->orient, h->phase,
+                  h->kr[2], h->kr[3], h->kr[4], h->kr[5], h->kr[6], h->spec, h->orient, h->phase,
                   h->gid, h->rm_tab, h->ktab, h->kvox, h->kvox_old, h->dparams,
                   h->g_buf[0], h->g_buf[1], h->g_old, h->ep_old, h->ep_trial, h->Gam_old,
                   h->Gam_trial, h->gam_old, h->gam_trial, h->partials, h->tickets,
@@ -689,6 +802,7 @@ static void free_handle(ssfft_handle *h) {
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->krylov_graph) cudaGraphExecDestroy(h->krylov_graph);
+  if (h->krylov_loop) cudaGraphExecDestroy(h->krylov_loop);
   if (h->h_results) cudaFreeHost(h->h_results);
   if (h->h_st) cudaFreeHost(h->h_st);
   if (h->h_cint) cudaFreeHost(h->h_cint);
@@ -734,7 +848,7 @@ extern "C" int ssfft_estimate_bytes(const ssfft_config *cfg, int any_evp, int n_
   const size_t V = (size_t)cfg->n[0] * cfg->n[1] * cfg->n[2];
   const size_t rs = cfg->precision == SSFFT_FP64 ? 8 : 4;
   const size_t S = (size_t)cfg->n[0] * cfg->n[1] * (cfg->n[2] / 2 + 1);
-  size_t b = 13 * 6 * V * rs + 6 * S * 16 + 3 * V * 4;
+  size_t b = 14 * 6 * V * rs + 6 * S * 16 + 3 * V * 4;
   if (any_evp) b += 2 * 21 * V * rs + (5 * (size_t)n_slip + 12 + 2) * V * 8;
   b += (size_t)MAX_PARTIAL_BLOCKS * 21 * 8 + (1 << 20);
   *bytes = b;
@@ -771,6 +885,8 @@ extern "C" int ssfft_create(const ssfft_config *cfg, ssfft_handle **out) {
     h->use_graphs = !(ng && ng[0] == '1');
     const char *np = getenv("SSFFT_NO_PLANE");
     h->use_plane = !(np && np[0] == '1');
+    const char *nl = getenv("SSFFT_NO_DEVICE_LOOP");
+    h->use_device_loop = h->use_graphs && !(nl && nl[0] == '1');
   }
   auto body = [&]() -> int {
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
@@ -805,7 +921,8 @@ extern "C" int ssfft_create(const ssfft_config *cfg, ssfft_handle **out) {
     CKR((set_kernel_attrs<float, float>(SMEM_LIMIT)));
     CKR((set_kernel_attrs<double, float>(SMEM_LIMIT)));
     void **fields[] = {&h->eps, &h->sig, &h->sig_old, &h->eps_old, &h->dfl, &h->guess, &h->b,
-                       &h->kr[0], &h->kr[1], &h->kr[2], &h->kr[3], &h->kr[4], &h->kr[5]};
+                       &h->kr[0], &h->kr[1], &h->kr[2], &h->kr[3], &h->kr[4], &h->kr[5],
+                       &h->kr[6]};
     for (void **f : fields) {
       ALLOC(*f, field_bytes(h, 6));
       CK(cudaMemsetAsync(*f, 0, field_bytes(h, 6), h->stream));
@@ -961,6 +1078,10 @@ static void drop_graph(ssfft_handle *h) {
   if (h->krylov_graph) {
     cudaGraphExecDestroy(h->krylov_graph);
     h->krylov_graph = nullptr;
+  }
+  if (h->krylov_loop) {
+    cudaGraphExecDestroy(h->krylov_loop);
+    h->krylov_loop = nullptr;
   }
 }
 
@@ -1356,55 +1477,30 @@ extern "C" int ssfft_timer(ssfft_handle *h, int start, double *seconds) {
 }
 
 template <typename T> static int profile_impl(ssfft_handle *h, int reps, double *sec) {
-  const long long n = 6 * h->V;
-  T *R1 = (T *)h->kr[0], *R2 = (T *)h->kr[1], *W = (T *)h->kr[2], *W1 = (T *)h->kr[3],
-    *W2 = (T *)h->kr[4], *X = (T *)h->kr[5];
+  KrylovBufs<T> k = krylov_bufs<T>(h);
   // a live MINRES state on the residual of the current stress (never marked done); call
   // after a solve so that the stress field is not uniform
   const double zero[6] = {0, 0, 0, 0, 0, 0};
   CKR(residual<T>(h, zero));
-  minres_init_kernel<T><<<h->red_blocks, SSFFT_THREADS, 0, h->stream>>>(
-      (const T *)h->b, R1, R2, X, W, W2, n, h->st, 0.0, (long long)1 << 60, h->partials,
-      h->tickets + TK_INIT);
-  CK(cudaGetLastError());
+  CKR(launch_minres_init<T>(h, k, 0.0, (long long)1 << 60));
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   NvtxScope range("ssfft_profile_krylov");  // only the timed Krylov kernels
   for (int r = 0; r < reps; ++r) {
-    ProArgs<T> pa{};
-    pa.in = R2;
-    pa.gid = h->gid;
-    pa.ktab = (const T *)h->ktab;
-    pa.kvox = (const T *)h->kvox;
-    pa.st = h->st;
-    EpiArgs<T> ea{};
-    ea.out = R1;
-    ea.r2 = R2;
-    ea.st = h->st;
-    ea.partials = h->partials;
-    ea.ticket = h->tickets + TK_ZINV;
-    if (h->voxel_mode)
-      CKR((launch_projector<T, T, PRO_TANGENT_VOXEL, EPI_MINRES>(h, pa, ea, h->st, h->pev)));
-    else
-      CKR((launch_projector<T, T, PRO_TANGENT_TABLE, EPI_MINRES>(h, pa, ea, h->st, h->pev)));
-    CKR(launch_update<T>(h, R1, R2, W2, W, W1, X));
+    CKR(krylov_iteration<T>(h, k, h->pev));
     CK(cudaEventRecord(h->pev[6], h->stream));
-    std::swap(R1, R2);
-    T *old_w1 = W1;
-    W1 = W2;
-    W2 = W;
-    W = old_w1;
+    k.advance();
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(h->pev[6]));
-    for (int k = 0; k < 6; ++k) {
+    for (int i = 0; i < 6; ++i) {
       float ms = 0.f;
-      CK(cudaEventElapsedTime(&ms, h->pev[k], h->pev[k + 1]));
-      acc[k] += ms * 1e-3;
+      CK(cudaEventElapsedTime(&ms, h->pev[i], h->pev[i + 1]));
+      acc[i] += ms * 1e-3;
     }
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, h->pev[0], h->pev[6]));
     acc[7] += ms * 1e-3;
   }
-  for (int k = 0; k < 8; ++k) sec[k] = acc[k] / reps;
+  for (int i = 0; i < 8; ++i) sec[i] = acc[i] / reps;
   sec[6] = 0.0;
   return 0;
 }
