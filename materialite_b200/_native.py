@@ -93,6 +93,7 @@ class SsfftSolveOut(ctypes.Structure):
         ("device_seconds", ctypes.c_double),
         ("mean_stress", ctypes.c_double * 6),
         ("mean_strain", ctypes.c_double * 6),
+        ("kernel_launches", ctypes.c_int64),
     ]
 
 

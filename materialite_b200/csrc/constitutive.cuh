@@ -46,6 +46,7 @@ template <typename T> struct ConstArgs {
   const int32_t *phase;    // phase per voxel (null: phase 0)
   const int32_t *orient;   // orientation per voxel
   const PhaseParams *params;
+  int n_params;            // phases staged in shared memory (highest phase id + 1)
   const double *rm_tab;    // [n_orient][36] Mandel rotations (specimen -> crystal)
   // EVP state (double, planes of V): g_in is read (previous trial), g_out written
   const double *g_in;
@@ -63,7 +64,8 @@ template <typename T> struct ConstArgs {
 };
 
 __device__ __forceinline__ void cholesky6(const double *M, double *L) {
-  // M, L packed symmetric (sym_idx); L holds the lower factor L[i][j], i >= j
+  // M, L packed symmetric (sym_idx); L holds the lower factor L[i][j], i >= j.  L may be
+  // M itself: entry (i, j) of M is read only before entry (i, j) of L is written.
 #pragma unroll
   for (int j = 0; j < 6; ++j) {
     double d = M[sym_idx(j, j)];
@@ -117,6 +119,27 @@ __device__ __forceinline__ double int_or_real_pow(double x, double e) {
   return pow(x, e);
 }
 
+// Increment of the slip resistance when it is the same for every system and independent
+// of the system's own value: perfect plasticity, linear and Voce hardening
+// (hardening_laws.py:18-72); g_new = g_old + this.
+__device__ __forceinline__ double harden_increment(const PhaseParams &P, double Gold,
+                                                   double dgam) {
+  switch (P.hardening) {
+    case HARD_LINEAR:
+      return P.props[0] * dgam;
+    case HARD_VOCE: {
+      const double tau1 = P.props[0], th0 = P.props[1], th1 = P.props[2];
+      const double ratio = fabs(th0 / tau1);
+      const double ei = exp(-ratio * Gold);
+      const double ec = exp(-ratio * dgam);
+      return th1 * dgam - (ratio * tau1 - th1) / ratio * ei * (ec - 1.0) -
+             th1 / ratio * ei * (ec * (1.0 + ratio * (Gold + dgam)) - 1.0 - ratio * Gold);
+    }
+    default:
+      return 0.0;
+  }
+}
+
 // Slip resistance of one system after an increment (hardening_laws.py:18-90).
 // dgam = dt * sum |gdot|; Gold = accumulated slip before the increment.
 __device__ __forceinline__ double harden_iso(const PhaseParams &P, double gold, double Gold,
@@ -147,11 +170,35 @@ __device__ __forceinline__ void load6(const T *f, long long V, long long v, doub
   for (int c = 0; c < 6; ++c) x[c] = (double)f[c * V + v];
 }
 
+// Threads of a constitutive block, and the shared memory a block holds: the phase table
+// plus per-thread slip arrays (old and current resistances, slip rates) and the two
+// crystal-frame strain vectors, [entry][thread] so that a warp's accesses are contiguous.
+#define CONST_THREADS 128
+inline size_t constitutive_smem_bytes(int n_params) {
+  return (size_t)n_params * sizeof(PhaseParams) +
+         (size_t)(3 * MAX_SLIP + 12) * CONST_THREADS * sizeof(double);
+}
+
 template <typename T>
-__global__ void __launch_bounds__(128) constitutive_kernel(ConstArgs<T> a) {
+__global__ void __launch_bounds__(CONST_THREADS, 3) constitutive_kernel(ConstArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char csm[];
+  PhaseParams *sp = reinterpret_cast<PhaseParams *>(csm);
+  const int tid = threadIdx.x;
+  double *s_gold = reinterpret_cast<double *>(sp + a.n_params) + tid;  // stride CONST_THREADS
+  double *s_gdot = s_gold + MAX_SLIP * CONST_THREADS;
+  double *s_g = s_gdot + MAX_SLIP * CONST_THREADS;
+  double *s_epo = s_g + MAX_SLIP * CONST_THREADS;
+  double *s_epc = s_epo + 6 * CONST_THREADS;
+#define TS(arr, k) arr[(k) * CONST_THREADS]
   __shared__ int blk_max;
   __shared__ int blk_fail;
-  if (threadIdx.x == 0) {
+  {
+    const int nw = a.n_params * (int)(sizeof(PhaseParams) / sizeof(int));
+    const int *src = reinterpret_cast<const int *>(a.params);
+    int *dst = reinterpret_cast<int *>(sp);
+    for (int i = tid; i < nw; i += CONST_THREADS) dst[i] = src[i];
+  }
+  if (tid == 0) {
     blk_max = 0;
     blk_fail = 0;
   }
@@ -159,10 +206,10 @@ __global__ void __launch_bounds__(128) constitutive_kernel(ConstArgs<T> a) {
   int my_iters = 0;
   bool my_fail = false;
   const long long V = a.V;
-  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < V;
-       v += (long long)gridDim.x * blockDim.x) {
+  for (long long v = (long long)blockIdx.x * CONST_THREADS + tid; v < V;
+       v += (long long)gridDim.x * CONST_THREADS) {
     const int ph = a.phase ? a.phase[v] : 0;
-    const PhaseParams &P = a.params[ph];
+    const PhaseParams &P = sp[ph];
     double eps[6];
     load6<T>(a.eps, V, v, eps);
     if (P.kind == PHASE_ELASTIC) {
@@ -198,27 +245,30 @@ __global__ void __launch_bounds__(128) constitutive_kernel(ConstArgs<T> a) {
 #pragma unroll
     for (int c = 0; c < 6; ++c) gnorm += gs[c] * gs[c];
     gnorm = sqrt(gnorm);
-    double sig[6], epc[6];
+    double sig[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
       double s0 = 0.0, e0 = 0.0;
 #pragma unroll
       for (int j = 0; j < 6; ++j) {
-        s0 += Rm[i * 6 + j] * gs[j];
-        e0 += Rm[i * 6 + j] * eps[j];
+        const double rij = Rm[i * 6 + j];
+        s0 += rij * gs[j];
+        e0 += rij * eps[j];
       }
       sig[i] = s0;
-      epc[i] = e0;
+      TS(s_epc, i) = e0;
+      TS(s_epo, i) = a.ep_old[i * V + v];
     }
     const int ns = P.nslip;
     const double dt = a.dt;
     const double Gold = a.Gam_old[v];
-    double g[MAX_SLIP], gdot[MAX_SLIP];
-#pragma unroll
-    for (int al = 0; al < MAX_SLIP; ++al) g[al] = (al < ns) ? a.g_in[al * V + v] : 1.0;
-    double epo[6];
-    load6<double>(a.ep_old, V, v, epo);
-    double ep[6], M[21], L[21];
+    for (int al = 0; al < ns; ++al) {
+      TS(s_g, al) = a.g_in[al * V + v];
+      TS(s_gold, al) = a.g_old[al * V + v];
+    }
+    // linear / Voce / perfect with no latent ratio: one increment for all systems
+    const bool iso = (P.latent == 1.0) && (P.hardening != HARD_AF);
+    double ep[6], M[21];
     double dgam = 0.0;
     bool conv = false;
     int it = 0;
@@ -226,55 +276,49 @@ __global__ void __launch_bounds__(128) constitutive_kernel(ConstArgs<T> a) {
       ++it;
       // slip rates at the current stress (elastic_viscoplastic.py:205-216)
 #pragma unroll
-      for (int c = 0; c < 6; ++c) ep[c] = epo[c];
+      for (int c = 0; c < 6; ++c) ep[c] = TS(s_epo, c);
 #pragma unroll
       for (int i = 0; i < 6; ++i)
 #pragma unroll
         for (int j = i; j < 6; ++j) M[sym_idx(i, j)] = P.Cinv[i * 6 + j];
       dgam = 0.0;
+      for (int al = 0; al < ns; ++al) {
+        const double *Pa = P.P + al * 6;
+        double pa[6];
 #pragma unroll
-      for (int al = 0; al < MAX_SLIP; ++al) {
-        if (al < ns) {
-          const double *Pa = P.P + al * 6;
-          double tau = 0.0;
+        for (int c = 0; c < 6; ++c) pa[c] = Pa[c];
+        double tau = 0.0;
 #pragma unroll
-          for (int c = 0; c < 6; ++c) tau += sig[c] * Pa[c];
-          const double ga = g[al];
-          const double pref = P.gdot0 * int_or_real_pow(fabs(tau / ga), P.n - 1.0) / ga;
-          const double gd = pref * tau;
-          gdot[al] = gd;
-          dgam += fabs(gd);
-          const double wep = dt * gd;
+        for (int c = 0; c < 6; ++c) tau += sig[c] * pa[c];
+        const double inv_g = 1.0 / TS(s_g, al);
+        const double pref = P.gdot0 * int_or_real_pow(fabs(tau) * inv_g, P.n - 1.0) * inv_g;
+        const double gd = pref * tau;
+        TS(s_gdot, al) = gd;
+        dgam += fabs(gd);
+        const double wep = dt * gd;
 #pragma unroll
-          for (int c = 0; c < 6; ++c) ep[c] += wep * Pa[c];
-          const double wm = dt * P.n * pref;
+        for (int c = 0; c < 6; ++c) ep[c] += wep * pa[c];
+        const double wm = dt * P.n * pref;
 #pragma unroll
-          for (int i = 0; i < 6; ++i)
+        for (int i = 0; i < 6; ++i) {
+          const double wi = wm * pa[i];
 #pragma unroll
-            for (int j = i; j < 6; ++j) M[sym_idx(i, j)] += wm * Pa[i] * Pa[j];
-        } else {
-          gdot[al] = 0.0;
+          for (int j = i; j < 6; ++j) M[sym_idx(i, j)] += wi * pa[j];
         }
       }
       dgam *= dt;
-      // Newton update sigma <- sigma - J^-1 (sigma - C (eps - ep))   (:225-235)
-      double r[6], cr[6], z[6];
+      // Newton update sigma <- sigma - J^-1 (sigma - C (eps - ep))   (:225-235), with
+      // J^-1 r = M^-1 C^-1 r and C^-1 r = C^-1 sigma - (eps - ep)
+      double cr[6], z[6];
 #pragma unroll
       for (int i = 0; i < 6; ++i) {
-        double acc = sig[i];
+        double acc = ep[i] - TS(s_epc, i);
 #pragma unroll
-        for (int j = 0; j < 6; ++j) acc -= P.C[i * 6 + j] * (epc[j] - ep[j]);
-        r[i] = acc;
-      }
-#pragma unroll
-      for (int i = 0; i < 6; ++i) {
-        double acc = 0.0;
-#pragma unroll
-        for (int j = 0; j < 6; ++j) acc += P.Cinv[i * 6 + j] * r[j];
+        for (int j = 0; j < 6; ++j) acc += P.Cinv[i * 6 + j] * sig[j];
         cr[i] = acc;
       }
-      cholesky6(M, L);
-      chol_solve6(L, cr, z);
+      cholesky6(M, M);
+      chol_solve6(M, cr, z);
       double diff = 0.0;
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
@@ -283,19 +327,19 @@ __global__ void __launch_bounds__(128) constitutive_kernel(ConstArgs<T> a) {
       }
       diff = sqrt(diff);
       // hardening (:236-242), from the state at the start of the increment
-      double tot = 0.0;
-      if (P.latent != 1.0) {
-#pragma unroll
-        for (int al = 0; al < MAX_SLIP; ++al) tot += fabs(gdot[al]);
-      }
-#pragma unroll
-      for (int al = 0; al < MAX_SLIP; ++al) {
-        if (al < ns) {
-          const double go = a.g_old[al * V + v];
+      if (iso) {
+        const double inc = harden_increment(P, Gold, dgam);
+        for (int al = 0; al < ns; ++al) TS(s_g, al) = TS(s_gold, al) + inc;
+      } else {
+        double tot = 0.0;
+        if (P.latent != 1.0)
+          for (int al = 0; al < ns; ++al) tot += fabs(TS(s_gdot, al));
+        for (int al = 0; al < ns; ++al) {
+          const double go = TS(s_gold, al);
           double gn = harden_iso(P, go, Gold, dgam);
           if (P.latent != 1.0 && tot > 0.0)
-            gn = go + (gn - go) * (P.latent * tot + (1.0 - P.latent) * fabs(gdot[al])) / tot;
-          g[al] = gn;
+            gn = go + (gn - go) * (P.latent * tot + (1.0 - P.latent) * fabs(TS(s_gdot, al))) / tot;
+          TS(s_g, al) = gn;
         }
       }
       conv = (diff / gnorm <= EVP_TOLERANCE) || (diff / P.E_ref < 1.0e-12);
@@ -306,17 +350,7 @@ __global__ void __launch_bounds__(128) constitutive_kernel(ConstArgs<T> a) {
       my_fail = true;
       continue;
     }
-    // tangent M^-1 in the crystal frame, then both back to the specimen frame
-    double Tc[21];
-#pragma unroll
-    for (int j = 0; j < 6; ++j) {
-      double e[6], col[6];
-#pragma unroll
-      for (int i = 0; i < 6; ++i) e[i] = (i == j) ? 1.0 : 0.0;
-      chol_solve6(L, e, col);
-#pragma unroll
-      for (int i = 0; i <= j; ++i) Tc[sym_idx(i, j)] = col[i];
-    }
+    // stress back to the specimen frame
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
       double acc = 0.0;
@@ -324,40 +358,49 @@ __global__ void __launch_bounds__(128) constitutive_kernel(ConstArgs<T> a) {
       for (int j = 0; j < 6; ++j) acc += Rm[j * 6 + i] * sig[j];
       a.sig[i * V + v] = (T)acc;
     }
-    // K_s = Rm^T Tc Rm
-    double TR[36];
+    // tangent M^-1 in the crystal frame (columns from the factor), then
+    // K_s = Rm^T M^-1 Rm one row at a time
+    double Tc[21];
 #pragma unroll
-    for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) {
+      double e[6], col[6];
 #pragma unroll
-      for (int b = 0; b < 6; ++b) {
+      for (int i = 0; i < 6; ++i) e[i] = (i == j) ? 1.0 : 0.0;
+      chol_solve6(M, e, col);
+#pragma unroll
+      for (int i = 0; i <= j; ++i) Tc[sym_idx(i, j)] = col[i];
+    }
+#pragma unroll
+    for (int p = 0; p < 6; ++p) {
+      double t[6];  // row p of Rm^T Tc
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
         double acc = 0.0;
 #pragma unroll
-        for (int j = 0; j < 6; ++j) acc += Tc[sym_idx(i, j)] * Rm[j * 6 + b];
-        TR[i * 6 + b] = acc;
+        for (int i = 0; i < 6; ++i) acc += Rm[i * 6 + p] * Tc[sym_idx(i, j)];
+        t[j] = acc;
       }
-#pragma unroll
-    for (int p = 0; p < 6; ++p)
 #pragma unroll
       for (int b = p; b < 6; ++b) {
         double acc = 0.0;
 #pragma unroll
-        for (int i = 0; i < 6; ++i) acc += Rm[i * 6 + p] * TR[i * 6 + b];
+        for (int j = 0; j < 6; ++j) acc += t[j] * Rm[j * 6 + b];
         a.kvox[sym_idx(p, b) * V + v] = (T)acc;
       }
-#pragma unroll
-    for (int al = 0; al < MAX_SLIP; ++al)
-      if (al < ns) {
-        a.g_out[al * V + v] = g[al];
-        if (a.gam_trial) a.gam_trial[al * V + v] = a.gam_old[al * V + v] + gdot[al] * dt;
-      }
+    }
+    for (int al = 0; al < ns; ++al) {
+      a.g_out[al * V + v] = TS(s_g, al);
+      if (a.gam_trial) a.gam_trial[al * V + v] = a.gam_old[al * V + v] + TS(s_gdot, al) * dt;
+    }
 #pragma unroll
     for (int c = 0; c < 6; ++c) a.ep_trial[c * V + v] = ep[c];
     a.Gam_trial[v] = Gold + dgam;
   }
+#undef TS
   if (my_iters) atomicMax(&blk_max, my_iters);
   if (my_fail) blk_fail = 1;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     atomicMax(a.max_iters, blk_max);
     if (blk_fail) atomicOr(a.failed, 1);
   }

@@ -168,7 +168,9 @@ __device__ __forceinline__ void prologue(const Grid<T> &g, const ProArgs<TF> &a,
 // (u_{j+1} = y' - coef u_j, w = (v_j - oldeps w1 - delta w2) denom, x += phi w, with
 // v_j = s_prev u_j), then tau = K (s u_{j+1}).  Every block forms all six components of
 // u_{j+1} (the tangent couples them) but updates and stores only the components it owns:
-// all six (PAIR < 0) or the pair 2 PAIR, 2 PAIR + 1; |x|^2 of those accumulates into xx.
+// all six (ALL) or the pair 2 pair, 2 pair + 1; |x|^2 of those accumulates into xx.  With
+// ALL, tau[0..5] is the whole tau; otherwise tau[0..1] are the owned pair's components,
+// and only the two tangent rows they need are loaded.
 template <typename T, typename TF, int PRO, bool ALL>
 __device__ __forceinline__ void tangent_prologue(const Grid<T> &g, const ProArgs<TF> &a,
                                                  long long v, const PendingUpdate<T> &u,
@@ -178,16 +180,26 @@ __device__ __forceinline__ void tangent_prologue(const Grid<T> &g, const ProArgs
   const long long V = g.V;
   // every load is issued before the first store: the stores may alias the loaded arrays
   // as far as the compiler knows, and loads held back behind them would serialise
-  T r[6], yv[6], a1[NO], a2[NO], xo[NO], k[21];
+  T r[6], yv[6], a1[NO], a2[NO], xo[NO], k[ALL ? 21 : 12];
 #pragma unroll
   for (int c = 0; c < 6; ++c) r[c] = (T)a.in[c * V + v];
+  const TF *kp;
+  long long ks;
   if constexpr (PRO == PRO_TANGENT_TABLE) {
-    const TF *kp = a.ktab + (long long)a.gid[v] * 21;
+    kp = a.ktab + (long long)a.gid[v] * 21;
+    ks = 1;
+  } else {
+    kp = a.kvox + v;
+    ks = V;
+  }
+  if constexpr (ALL) {
 #pragma unroll
-    for (int q = 0; q < 21; ++q) k[q] = (T)kp[q];
+    for (int q = 0; q < 21; ++q) k[q] = (T)kp[q * ks];
   } else {
 #pragma unroll
-    for (int q = 0; q < 21; ++q) k[q] = (T)a.kvox[q * V + v];
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+      for (int j = 0; j < 6; ++j) k[q * 6 + j] = (T)kp[sym_idx(c0 + q, j) * ks];
   }
   if (u.on) {
 #pragma unroll
@@ -231,7 +243,17 @@ __device__ __forceinline__ void tangent_prologue(const Grid<T> &g, const ProArgs
 #pragma unroll
     for (int c = 0; c < 6; ++c) vv[c] = u.s * r[c];
   }
-  sym6_apply<T>(k, 1, vv, tau);
+  if constexpr (ALL) {
+    sym6_apply<T>(k, 1, vv, tau);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      T acc = 0;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) acc += k[q * 6 + j] * vv[j];
+      tau[q] = acc;
+    }
+  }
 }
 
 // End of a forward pass that applied a pending update: |x|^2 over all blocks, then the
@@ -648,11 +670,13 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
   const long long vbase = (long long)x * ny * nz;
   for (int e = threadIdx.x; e < ny * nz; e += blockDim.x) {
     T tau[6];
-    if constexpr (PRO >= PRO_TANGENT_TABLE)
+    if constexpr (PRO >= PRO_TANGENT_TABLE) {
       tangent_prologue<T, TF, PRO, false>(g, a, vbase + e, u, p, tau, xx);
-    else
+      bufA[sidx<true>(e)] = mk<T>(tau[0], tau[1]);
+    } else {
       prologue<T, TF, PRO>(g, a, vbase + e, (T)1, tau);
-    bufA[sidx<true>(e)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
+      bufA[sidx<true>(e)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
+    }
   }
   __syncthreads();
   const LineLayout Lz(ny, ny, 0, nz, 1);

@@ -220,6 +220,7 @@ template <typename T, typename TF> static int set_kernel_attrs(size_t smax) {
   CKR((plane_attrs<T, TF, 512>(m)));
   CKR((plane_attrs<T, TF, 1024>(m)));
   if (sizeof(T) == sizeof(TF)) {
+    CKR(smem_attr(constitutive_kernel<T>, (int)constitutive_smem_bytes(SSFFT_MAX_PHASES)));
     CKR(smem_attr(zfwd_kernel<T, T, PRO_TANGENT_TABLE>, m));
     CKR(smem_attr(zfwd_kernel<T, T, PRO_TANGENT_VOXEL>, m));
     CKR(smem_attr(zinv_kernel<T, T, EPI_MINRES>, m));
@@ -571,6 +572,9 @@ static int constitutive(ssfft_handle *h, double dt) {
   a.phase = phase_ptr(h);
   a.orient = h->orient;
   a.params = h->dparams;
+  a.n_params = 1;
+  for (int p = 0; p < SSFFT_MAX_PHASES; ++p)
+    if (h->phase_set[p]) a.n_params = p + 1;
   a.rm_tab = h->rm_tab;
   if (h->any_evp) {
     a.g_in = h->g_buf[h->g_cur];
@@ -586,8 +590,9 @@ static int constitutive(ssfft_handle *h, double dt) {
   a.dt = dt;
   a.max_iters = h->citers;
   a.failed = h->cfail;
-  const int blocks = std::max(1, std::min(div_up(h->V, 128), 148 * 16));
-  constitutive_kernel<T><<<blocks, 128, 0, h->stream>>>(a);
+  const int blocks = std::max(1, std::min(div_up(h->V, CONST_THREADS), 148 * 16));
+  constitutive_kernel<T><<<blocks, CONST_THREADS, constitutive_smem_bytes(a.n_params),
+                           h->stream>>>(a);
   h->launches += 1;
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(h->h_cint, h->citers, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -1283,6 +1288,12 @@ extern "C" int ssfft_solve_constant_rates(ssfft_handle *h, const ssfft_rate_sche
   if (!h || !sc || !out) return fail(SSFFT_E_INVALID, "null argument");
   if (!h->micro_set) return fail(SSFFT_E_INVALID, "microstructure not set");
   memset(out, 0, sizeof(*out));
+  struct LaunchTally {  // kernel launches of this solve, on every return path
+    ssfft_handle *h;
+    ssfft_solve_out *o;
+    long long l0;
+    ~LaunchTally() { o->kernel_launches = h->launches - l0; }
+  } tally{h, out, h->launches};
   const double *mask = h->cfg.stress_mask;
   double er[6], sr[6];
   for (int c = 0; c < 6; ++c) {  // apply_stress_mask (load_schedule.py:26-30)

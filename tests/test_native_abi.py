@@ -70,3 +70,42 @@ def test_config_validation(n, mask, code):
 def test_invalid_precision_rejected():
     rc, _ = estimate(config(precision=7))
     assert rc == -1
+
+
+# ctypes mirrors of the header's structs, with their C type names
+def _struct_mirrors():
+    from materialite_b200 import serving as sv
+    return {"ssfft_config": nat.SsfftConfig, "ssfft_step_in": nat.SsfftStepIn,
+            "ssfft_step_out": nat.SsfftStepOut, "ssfft_rate_schedule": nat.SsfftRateSchedule,
+            "ssfft_solve_out": nat.SsfftSolveOut, "ssfft_phase": sv.SsfftPhase,
+            "ssfft_request": sv.SsfftRequest, "ssfft_completion": sv.SsfftCompletion}
+
+
+def test_ctypes_structs_match_the_header_layout(tmp_path):
+    """Size and every field offset of each ctypes struct equal what a C compiler makes
+    of include/ssfft.h (gcc on the host; no GPU)."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    mirrors = _struct_mirrors()
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', 'int main(void) {']
+    for cname, py in mirrors.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append('  return 0;\n}')
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([gcc, "-std=c11", str(src), "-o", str(exe)], check=True)
+    got = {}
+    for row in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n"):
+        if row:
+            cname, key, val = row.split()
+            got[(cname, key)] = int(val)
+    for cname, py in mirrors.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
