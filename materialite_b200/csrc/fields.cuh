@@ -107,12 +107,26 @@ __device__ __forceinline__ double dev_norm6(const double *s) {
 //   out[0..5]  sum of stress      out[6..11] sum of strain
 //   out[12]    max |dev(stress - old_stress)|   out[13] max |K : dx|  (if dx given)
 #define NORM_VALS 14
+#define NORM_SUMS 12  // values 0..11 are sums, 12..13 maxima
+
+// Combine one of the norm values (sum or max) in a fixed order.
+__device__ __forceinline__ double norm_combine(int k, double a, double b) {
+  return k < NORM_SUMS ? a + b : fmax(a, b);
+}
+
+// Warp tree reduction of value k (fixed shuffle order).
+__device__ __forceinline__ double norm_warp_reduce(int k, double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = norm_combine(k, v, __shfl_down_sync(0xffffffffu, v, off));
+  return v;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(SSFFT_THREADS)
     newton_norms_kernel(long long V, const T *__restrict__ sig, const T *__restrict__ sig_old,
                         const T *__restrict__ eps, const T *__restrict__ dx, TangentRef<T> K,
                         double *partials, unsigned int *ticket, double *out) {
-  __shared__ double red[32];
+  __shared__ double wred[NORM_VALS][SSFFT_THREADS / 32];
   double acc[NORM_VALS];
 #pragma unroll
   for (int k = 0; k < NORM_VALS; ++k) acc[k] = 0.0;
@@ -138,16 +152,28 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
       acc[13] = fmax(acc[13], sqrt(n2));
     }
   }
+  // all fourteen values through one warp pass and one barrier
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
   for (int k = 0; k < NORM_VALS; ++k) {
-    const double r = (k < 12) ? block_sum(acc[k], red) : block_max(acc[k], red);
-    if (threadIdx.x == 0) partials[(size_t)blockIdx.x * NORM_VALS + k] = r;
+    const double r = norm_warp_reduce(k, acc[k]);
+    if (lane == 0) wred[k][warp] = r;
+  }
+  __syncthreads();
+  if (threadIdx.x < NORM_VALS) {
+    const int k = threadIdx.x;
+    double r = wred[k][0];
+    for (int w = 1; w < nw; ++w) r = norm_combine(k, r, wred[k][w]);
+    partials[(size_t)blockIdx.x * NORM_VALS + k] = r;
   }
   if (!last_block_arrives(ticket)) return;
-  for (int k = 0; k < NORM_VALS; ++k) {
-    const double r = (k < 12) ? ordered_sum(partials + k, gridDim.x, NORM_VALS, red)
-                              : ordered_max(partials + k, gridDim.x, NORM_VALS, red);
-    if (threadIdx.x == 0) out[k] = r;
+  // one warp per value: lanes stride over the block partials, then a fixed tree
+  for (int k = warp; k < NORM_VALS; k += nw) {
+    double r = 0.0;
+    for (int b = lane; b < (int)gridDim.x; b += 32)
+      r = norm_combine(k, r, partials[(size_t)b * NORM_VALS + k]);
+    r = norm_warp_reduce(k, r);
+    if (lane == 0) out[k] = r;
   }
   if (threadIdx.x == 0) *ticket = 0;
 }

@@ -278,8 +278,11 @@ __device__ __forceinline__ void load_table(cplx<T> *dst, const cplx<T> *src, int
 
 // zfwd: blockIdx.x covers g.lz consecutive (x,y) lines.  TF is the storage type of the
 // input fields (TF = T except when a double-precision transform reads float fields).
+// z kernels: three blocks per SM in float (80 registers), two in double
+#define Z_MIN_BLOCKS(T) (sizeof(T) == 4 ? 3 : 2)
+
 template <typename T, typename TF, int PRO>
-__global__ void __launch_bounds__(SSFFT_THREADS)
+__global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
     zfwd_kernel(Grid<T> g, ProArgs<TF> a, cplx<T> *__restrict__ spec) {
   if (PRO >= PRO_TANGENT_TABLE && a.st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -403,8 +406,9 @@ __device__ __forceinline__ void green_apply(const Grid<T> &g, int kx, int ky, in
 
 // x pass: grid (ceil(hz/kx), ny); forward x-FFT of all six components, Gamma-hat,
 // inverse x-FFT, store.
+#define XPASS_THREADS SSFFT_THREADS
 template <typename T>
-__global__ void __launch_bounds__(SSFFT_THREADS)
+__global__ void __launch_bounds__(XPASS_THREADS)
     xpass_kernel(Grid<T> g, cplx<T> *__restrict__ spec, const MinresState *st) {
   if (st && st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -499,7 +503,7 @@ static __device__ __noinline__ void minres_after_matvec(MinresState *st, double 
 #define EPI_BATCH 4      // plane epilogue: elements per thread whose loads go out together
 
 template <typename T, typename TF, int EPI>
-__global__ void __launch_bounds__(SSFFT_THREADS)
+__global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
     zinv_kernel(Grid<T> g, EpiArgs<TF> a, const cplx<T> *__restrict__ spec) {
   if (EPI == EPI_MINRES && a.st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -286,7 +286,7 @@ static int launch_projector(ssfft_handle *h, const ProArgs<TF> &pa, const EpiArg
       zyfwd_kernel<T, TF, PRO, 512><<<dim3(h->nx, 3), 512, sp, h->stream>>>(g, pa, spec);
     rec(1);
     rec(2);
-    xpass_kernel<T><<<dim3(div_up(h->hz, h->kx), h->ny), SSFFT_THREADS, sx, h->stream>>>(
+    xpass_kernel<T><<<dim3(div_up(h->hz, h->kx), h->ny), XPASS_THREADS, sx, h->stream>>>(
         g, spec, st);
     rec(3);
     rec(4);
@@ -305,7 +305,7 @@ static int launch_projector(ssfft_handle *h, const ProArgs<TF> &pa, const EpiArg
     ypass_kernel<T, false><<<dim3(div_up(h->hz, h->ky), h->nx, 6), SSFFT_THREADS, sy,
                              h->stream>>>(g, spec, st);
     rec(2);
-    xpass_kernel<T><<<dim3(div_up(h->hz, h->kx), h->ny), SSFFT_THREADS, sx, h->stream>>>(
+    xpass_kernel<T><<<dim3(div_up(h->hz, h->kx), h->ny), XPASS_THREADS, sx, h->stream>>>(
         g, spec, st);
     rec(3);
     ypass_kernel<T, true><<<dim3(div_up(h->hz, h->ky), h->nx, 6), SSFFT_THREADS, sy,
@@ -608,7 +608,9 @@ static void constitutive_result(ssfft_handle *h, int *iters, int *failed) {
 }
 
 template <typename T> static int norms(ssfft_handle *h, const T *dx) {
-  newton_norms_kernel<T><<<h->red_blocks, SSFFT_THREADS, 0, h->stream>>>(
+  // about four points per thread: the fourteen block partials are cheap to combine
+  const int nb = std::max(1, std::min(div_up(h->V, 4 * SSFFT_THREADS), 2 * 148));
+  newton_norms_kernel<T><<<nb, SSFFT_THREADS, 0, h->stream>>>(
       h->V, (const T *)h->sig, (const T *)h->sig_old, (const T *)h->eps, dx, tangent_ref<T>(h),
       h->partials, h->tickets + TK_NORMS, h->results);
   h->launches += 1;
