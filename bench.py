@@ -41,6 +41,14 @@ WORKLOADS = {
                   precision="mixed", seed=0, model="evp"),
     "evp96": dict(n=96, grains=200, steps=5, dt=0.2, rate=1e-3, gtol=1e-6, ltol=1e-5,
                   precision="mixed", seed=0, model="evp"),
+    # Crystal EVP plain GPU solve: FCC, Voce 0.1/0.3/1.0, latent ratio 1.4, 64^3, 200
+    # grains, uniaxial x 1e-3 to 2% strain in 100 steps.
+    "evp64_latent": dict(n=64, grains=200, steps=100, dt=0.2, rate=1e-3, gtol=1e-6,
+                         ltol=1e-5, precision="mixed", seed=0, model="evp", latent=1.4),
+    # Two-phase large RVE: 256^3, 2000 grains, each grain EVP (as above, latent 1) or cubic
+    # elastic x10 with probability 1/2, uniaxial x 1e-3 to 1% strain in 50 steps.
+    "twophase256": dict(n=256, grains=2000, steps=50, dt=0.2, rate=1e-3, gtol=1e-6,
+                        ltol=1e-5, precision="mixed", seed=0, model="twophase"),
     # Serving stream: requests with N ~ U{32,48,64,96}, 20-400 periodic Voronoi grains,
     # elastic or FCC EVP (p = 1/2), uniaxial or biaxial strain rate 1e-3, 10-50 steps,
     # Poisson arrivals; the first `count` requests of the seeded stream.
@@ -92,6 +100,15 @@ def build_microstructure(w):
     ids = periodic_voronoi((n, n, n), w["grains"], rng)
     rot = quaternion_random_rotations(w["grains"], rng)
     return rot, ids.astype(np.int32)
+
+
+def phase_of_points(w, ids):
+    """Two-phase workloads: phase 0 (EVP) or 1 (elastic x10) per grain with probability
+    1/2, drawn from the workload's seed after the microstructure."""
+    if w.get("model") != "twophase":
+        return None
+    rng = np.random.default_rng(w["seed"] + 1)
+    return (rng.random(w["grains"]) < 0.5).astype(np.int32)[ids]
 
 
 def uniaxial_x(rate):
@@ -159,18 +176,21 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_handle(w, rot, ids, device):
+def make_handle(w, rot, ids, device, precision=None):
     from materialite_b200.engine import PhaseSpec, SolverHandle
     from materialite_b200.serving import evp_phase
     mask, *_ = uniaxial_x(w["rate"])
     n = w["n"]
-    h = SolverHandle((n, n, n), mask, w["precision"], global_tolerance=w["gtol"],
+    h = SolverHandle((n, n, n), mask, precision or w["precision"], global_tolerance=w["gtol"],
                      linear_solver_tolerance=w["ltol"], device=device)
+    elastic = PhaseSpec("elastic", cubic_mandel(250.0, 150.0, 120.0))
     if w.get("model") == "evp":
-        h.set_phases([evp_phase()])
+        h.set_phases([evp_phase(w.get("latent", 1.0))])
+    elif w.get("model") == "twophase":
+        h.set_phases([evp_phase(), PhaseSpec("elastic", cubic_mandel(250.0, 150.0, 120.0) * 10)])
     else:
-        h.set_phases([PhaseSpec("elastic", cubic_mandel(250.0, 150.0, 120.0))])
-    h.set_microstructure(rot, ids)
+        h.set_phases([elastic])
+    h.set_microstructure(rot, ids, phase_of_points(w, ids))
     return h
 
 
@@ -476,6 +496,41 @@ def kernels_mode(args, w):
     print(json.dumps(out), flush=True)
 
 
+def accuracy_mode(args, w):
+    """One full solve of the workload in mixed precision and in FP64 on the same inputs:
+    device seconds, iteration counts and the mixed stress field's relative L2 error
+    against FP64 (the size-independent check at sizes the oracle cannot reach; the FP64
+    path itself is pinned to the oracle at small sizes)."""
+    from materialite_b200.engine import SolveStats
+    if args.load_steps:
+        w = dict(w, steps=args.load_steps)
+    rot, ids = build_microstructure(w)
+    out = {"workload": args.workload, "n": w["n"], "steps": w["steps"]}
+    stress = {}
+    for prec in ("mixed", "fp64"):
+        h = make_handle(w, rot, ids, 0, precision=prec)
+        st = SolveStats()
+        h.timer_start()
+        res, _ = run_solve(h, w, st)
+        t = h.timer_stop()
+        stress[prec] = res["stress"]
+        out[prec] = {"device_s": t, "steps": st.steps, "cutbacks": getattr(st, "cutbacks", None),
+                     "newton": int(sum(st.newton_iterations)),
+                     "krylov": int(sum(st.krylov_iterations)),
+                     "mean_stress_xx": float(res["stress"][:, 0].mean())}
+        h.close()
+        print(json.dumps({prec: out[prec]}), flush=True)
+    a, b = stress["mixed"], stress["fp64"]
+    out["stress_rel_l2_mixed_vs_fp64"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    print(json.dumps(out), flush=True)
+
+
+# DRAM read + write bytes of one steady-state zfwd launch on plain128, from an ncu
+# --set full capture of `--mode kernels --workload plain128`: 260.3 MB read + 162.4 MB
+# written (algorithmic 462 MB).
+ZFWD_PLAIN128_TRAFFIC_BYTES = 422.6e6
+
+
 def plain128_roofline(device):
     """Roofline of the dominant Krylov kernel on the 128^3 plain solve (the HBM-bound
     regime), timed live with CUDA events on the handle's stream."""
@@ -494,7 +549,9 @@ def plain128_roofline(device):
     achieved = bpv[dom] * V / per_kernel[dom] / 1e9
     return {"bound": "hbm", "workload": "plain128 Krylov iteration", "kernel": dom,
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "peak_kind": kind,
+            "traffic": ZFWD_PLAIN128_TRAFFIC_BYTES if dom == "zfwd" else None,
+            "traffic_unit": "bytes per launch (ncu capture)",
+            "algorithmic_bytes": bpv[dom] * V, "peak_kind": kind,
             "per_kernel_us": {k: v * 1e6 for k, v in per_kernel.items()},
             "krylov_iteration_us": prof[7] * 1e6,
             "krylov_iteration_gbs": sum(bpv.values()) * V / prof[7] / 1e9}
@@ -509,10 +566,15 @@ def main():
     ap.add_argument("--workload", default="serve", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--mode", default="bench", choices=["bench", "kernels", "request"],
+    ap.add_argument("--mode", default="bench",
+                    choices=["bench", "kernels", "request", "accuracy"],
                     help="kernels: one load increment, then the Krylov kernels timed in "
-                         "isolation (the target of the ncu captures under profiles/)")
+                         "isolation (the target of the ncu captures under profiles/); "
+                         "request: one request of the serving stream alone; accuracy: one "
+                         "solve of the workload in mixed and in FP64, stress error between")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--load-steps", type=int, default=0,
+                    help="accuracy: solve only the first N load increments of the workload")
     ap.add_argument("--count", type=int, default=0, help="serve: number of requests")
     ap.add_argument("--no-roofline", action="store_true")
     ap.add_argument("--tag", type=int, default=0, help="request mode: index in the stream")
@@ -521,6 +583,9 @@ def main():
     w = WORKLOADS[args.workload]
     if args.mode == "kernels":
         kernels_mode(args, w)
+        return
+    if args.mode == "accuracy":
+        accuracy_mode(args, w)
         return
     if args.mode == "request":
         request_mode(args, WORKLOADS["serve"])
@@ -609,7 +674,9 @@ def main():
             "clocks": clocks,
             "gpu_launches": int(launches1 - launches0),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": (ZFWD_PLAIN128_TRAFFIC_BYTES
+                                     if args.workload == "plain128" and dom == "zfwd" else None),
                          "peak_kind": peak_kind,
                          "per_kernel_us": {k: v * 1e6 for k, v in per_kernel.items()},
                          "krylov_iteration_us": prof[7] * 1e6,
