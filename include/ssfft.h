@@ -60,6 +60,8 @@ extern "C" {
 #define SSFFT_FIELD_PLASTIC_STRAINS 3   /* (V,6) committed, specimen frame */
 #define SSFFT_FIELD_SLIP_SHEAR_STRAINS 4 /* (V,S) trial values of the last constitutive call */
 #define SSFFT_FIELD_RESIDUAL 5          /* (V,6) last equilibrium residual b */
+#define SSFFT_FIELD_YIELD_STRESSES 6    /* (V,1) J2 yield stresses, trial values of the last call */
+#define SSFFT_FIELD_EQ_PLASTIC_STRAINS 7 /* (V,1) J2 equivalent plastic strains, trial values */
 
 typedef struct ssfft_handle ssfft_handle;
 
@@ -126,6 +128,15 @@ int ssfft_set_phase_evp(ssfft_handle *h, int phase, const double stiffness[36], 
                         const double *schmid, double reference_slip_rate,
                         double rate_exponent, double slip_resistance, int hardening,
                         const double *hardening_props, int n_props, double latent_ratio);
+/* J2 small-strain plasticity, IsotropicElasticPlastic(modulus, shear_modulus,
+ * yield_stress, hardening_function, hardening_properties)
+ * (isotropic_elastic_plastic.py:17-53): isotropic elasticity, radial return with the
+ * reference's fixed-point iteration (tolerance 1e-7 on the equivalent plastic strain
+ * increment, at most 100 iterations, all points iterated until all have converged).  The
+ * hardening laws take the equivalent plastic strain rate as their single slip rate. */
+int ssfft_set_phase_j2(ssfft_handle *h, int phase, double modulus, double shear_modulus,
+                       double yield_stress, int hardening, const double *hardening_props,
+                       int n_props);
 
 /* Microstructure: n_orient unique rotations (n_orient x 9) and per-point indices into
  * them and into the phase table (phase_of_point may be NULL for a single phase 0).

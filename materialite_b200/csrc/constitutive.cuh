@@ -22,7 +22,7 @@
 #define EVP_MAX_ITERATIONS 60
 #define MAX_SLIP 12
 
-enum { PHASE_ELASTIC = 0, PHASE_EVP = 1 };
+enum { PHASE_ELASTIC = 0, PHASE_EVP = 1, PHASE_J2 = 2 };
 enum { HARD_PERFECT = 0, HARD_LINEAR = 1, HARD_VOCE = 2, HARD_AF = 3 };
 
 struct PhaseParams {
@@ -33,6 +33,7 @@ struct PhaseParams {
   double gdot0, n, g0, latent;
   double props[4];
   double E_ref;
+  double shear, bulk;  // J2: shear and bulk moduli (g0 is the initial yield stress)
 };
 
 template <typename T> struct ConstArgs {
@@ -61,6 +62,7 @@ template <typename T> struct ConstArgs {
   double dt;
   int *max_iters;          // atomicMax of iterations
   int *failed;             // set when a voxel does not converge
+  const int *j2;           // J2: [0] return-mapping iterations of every point, [1] any plastic
 };
 
 __device__ __forceinline__ void cholesky6(const double *M, double *L) {
@@ -170,6 +172,99 @@ __device__ __forceinline__ void load6(const T *f, long long V, long long v, doub
   for (int c = 0; c < 6; ++c) x[c] = (double)f[c * V + v];
 }
 
+// ---------------- J2 plasticity (isotropic_elastic_plastic.py:71-164) ----------------
+#define J2_TOLERANCE 1.0e-7
+#define J2_MAX_ITERATIONS 100
+
+// Elastic predictor of one point: deviatoric stress s (Mandel), mean stress, von Mises q.
+__device__ __forceinline__ void j2_predictor(const PhaseParams &P, const double *eps,
+                                             const double *ep_old, double *s, double &mean,
+                                             double &q) {
+  double ee[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) ee[c] = eps[c] - ep_old[c];
+  const double tr = ee[0] + ee[1] + ee[2];
+  const double vol = 1.0 / 3.0 * tr;  // tensor.py:1242-1244
+  double n2 = 0.0;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    s[c] = 2.0 * P.shear * (c < 3 ? ee[c] - vol : ee[c]);
+    n2 += s[c] * s[c];
+  }
+  mean = P.bulk * tr;
+  q = sqrt(1.5) * sqrt(n2);
+}
+
+// Yield stress after an equivalent plastic strain increment dp, as the reference calls the
+// hardening laws from IsotropicElasticPlastic: rate dp / dt, increment dt |rate|
+// (hardening_laws.py:35-38, 49-52, 83-86).
+__device__ __forceinline__ double j2_yield(const PhaseParams &P, double eq_old, double y_old,
+                                           double dp, double dt) {
+  return harden_iso(P, y_old, eq_old, dt * fabs(dp / dt));
+}
+
+// One fixed-point update of the return mapping (:110-119): residual clipped at zero,
+// inverse Jacobian -1/(3G).
+__device__ __forceinline__ double j2_update(const PhaseParams &P, double q, double dp,
+                                            double y) {
+  double r = q - 3.0 * P.shear * dp - y;
+  if (r <= 0.0) r = 0.0;
+  const double jinv = -1.0 / (3.0 * P.shear);
+  return dp - jinv * r;
+}
+
+// Pass 1 of a J2 update: the reference iterates every point until all have converged, so
+// each point's own iteration count is found first and reduced to the maximum (j2[0]),
+// with j2[1] = 1 if any point is plastic.  A point that does not converge within
+// J2_MAX_ITERATIONS fails the update (:133-137).
+template <typename T>
+__global__ void __launch_bounds__(SSFFT_THREADS) j2_count_kernel(ConstArgs<T> a, int *j2) {
+  __shared__ int blk_n, blk_any, blk_fail;
+  if (threadIdx.x == 0) {
+    blk_n = 0;
+    blk_any = 0;
+    blk_fail = 0;
+  }
+  __syncthreads();
+  int my_n = 0, my_any = 0, my_fail = 0;
+  const long long V = a.V;
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < V;
+       v += (long long)gridDim.x * blockDim.x) {
+    const PhaseParams &P = a.params[a.phase ? a.phase[v] : 0];
+    if (P.kind != PHASE_J2) continue;
+    double eps[6], epo[6], s[6], mean, q;
+    load6<T>(a.eps, V, v, eps);
+    load6<double>(a.ep_old, V, v, epo);
+    j2_predictor(P, eps, epo, s, mean, q);
+    const double y_old = a.g_old[v], eq_old = a.Gam_old[v];
+    if (!(q <= y_old)) my_any = 1;
+    double dp = 0.0, y = y_old;
+    int it = 0;
+    bool conv = false;
+    while (it < J2_MAX_ITERATIONS) {
+      ++it;
+      const double prev = dp;
+      dp = j2_update(P, q, dp, y);
+      y = j2_yield(P, eq_old, y_old, dp, a.dt);
+      if (fabs(dp - prev) < J2_TOLERANCE) {
+        conv = true;
+        break;
+      }
+    }
+    my_n = max(my_n, it);
+    if (!conv) my_fail = 1;
+  }
+  if (my_n) atomicMax(&blk_n, my_n);
+  if (my_any) blk_any = 1;
+  if (my_fail) blk_fail = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (blk_n) atomicMax(&j2[0], blk_n);
+    if (blk_any) atomicOr(&j2[1], 1);
+    if (blk_fail) atomicOr(a.failed, 1);
+  }
+}
+
 // Threads of a constitutive block, and the shared memory a block holds: the phase table
 // plus per-thread slip arrays (old and current resistances, slip rates) and the two
 // crystal-frame strain vectors, [entry][thread] so that a warp's accesses are contiguous.
@@ -235,6 +330,63 @@ __global__ void __launch_bounds__(CONST_THREADS, 3) constitutive_kernel(ConstArg
 #pragma unroll
       for (int c = 0; c < 6; ++c) a.sig[c * V + v] = (T)s[c];
       my_iters = max(my_iters, 1);
+      continue;
+    }
+    if (P.kind == PHASE_J2) {
+      // pass 2: every point runs the common iteration count of pass 1 (:106-138)
+      double epo[6], s[6], mean, q;
+      load6<double>(a.ep_old, V, v, epo);
+      j2_predictor(P, eps, epo, s, mean, q);
+      const double y_old = a.g_old[v], eq_old = a.Gam_old[v];
+      const bool elastic = q <= y_old;
+      double sig[6];
+      if (!a.j2[1]) {
+        // every point elastic: elastic stress, elastic tangent, state untouched (:94-99);
+        // the current slip-resistance plane is carried into the next trial buffer
+#pragma unroll
+        for (int c = 0; c < 6; ++c) sig[c] = s[c] + (c < 3 ? mean : 0.0);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) a.sig[c * V + v] = (T)sig[c];
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+          for (int j = i; j < 6; ++j) a.kvox[sym_idx(i, j) * V + v] = (T)P.C[i * 6 + j];
+        a.g_out[v] = a.g_in[v];
+        my_iters = max(my_iters, 1);
+        continue;
+      }
+      const int N = a.j2[0];
+      double dp = 0.0, y = y_old;
+      for (int it = 0; it < N; ++it) {
+        dp = j2_update(P, q, dp, y);
+        y = j2_yield(P, eq_old, y_old, dp, a.dt);
+      }
+      my_iters = max(my_iters, N);
+      // state (:139-146); a point with no deviatoric strain keeps its plastic strain
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        const double rs = q > 0.0 ? s[c] / q : 0.0;
+        a.ep_trial[c * V + v] = epo[c] + 1.5 * rs * dp;
+      }
+      a.Gam_trial[v] = eq_old + dp;
+      a.g_out[v] = y;
+      const double ratio = 3.0 * P.shear / q;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) sig[c] = (1.0 - ratio * dp) * s[c] + (c < 3 ? mean : 0.0);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) a.sig[c * V + v] = (T)sig[c];
+      // consistent tangent C - t1 I_dev + t2 s (x) s on plastic points, C on elastic ones
+      // (:148-163)
+      const double t1 = elastic ? 0.0 : 2.0 * P.shear * ratio * dp;
+      const double t2 = elastic ? 0.0 : ratio * ratio * (dp / q - 1.0 / (3.0 * P.shear));
+#pragma unroll
+      for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int j = i; j < 6; ++j) {
+          const double idev = (i == j ? 1.0 : 0.0) - (i < 3 && j < 3 ? 1.0 / 3.0 : 0.0);
+          const double k = elastic ? P.C[i * 6 + j] : P.C[i * 6 + j] - t1 * idev + t2 * (s[i] * s[j]);
+          a.kvox[sym_idx(i, j) * V + v] = (T)k;
+        }
       continue;
     }
     // ---------------- crystal elasto-viscoplasticity ----------------

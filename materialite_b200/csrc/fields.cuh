@@ -231,14 +231,21 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
   }
 }
 
-// Committed crystal-frame plastic strains -> specimen frame, point-major
-// (elastic_viscoplastic.py:258-263).
+// Committed plastic strains -> specimen frame, point-major: crystal-frame EVP strains are
+// rotated (elastic_viscoplastic.py:258-263); J2 strains are kept in the specimen frame.
 __global__ void __launch_bounds__(SSFFT_THREADS)
     plastic_to_specimen_kernel(long long V, const double *__restrict__ ep,
                                const int32_t *__restrict__ orient,
-                               const double *__restrict__ rm_tab, double *__restrict__ dst) {
+                               const double *__restrict__ rm_tab,
+                               const int32_t *__restrict__ phase,
+                               const PhaseParams *__restrict__ params, double *__restrict__ dst) {
   for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < V;
        v += (long long)gridDim.x * blockDim.x) {
+    if (params[phase ? phase[v] : 0].kind == PHASE_J2) {
+#pragma unroll
+      for (int i = 0; i < 6; ++i) dst[v * 6 + i] = ep[i * V + v];
+      continue;
+    }
     const double *Rm = rm_tab + (long long)orient[v] * 36;
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
@@ -250,7 +257,8 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
   }
 }
 
-// Initial EVP state: slip resistances g0 on EVP voxels, zero elsewhere.
+// Initial plastic state: slip resistances g0 on EVP voxels, the initial yield stress in
+// plane 0 on J2 voxels, zero elsewhere.
 __global__ void __launch_bounds__(SSFFT_THREADS)
     evp_init_kernel(long long V, int nslip_max, const int32_t *__restrict__ phase,
                     const PhaseParams *__restrict__ params, double *g_a, double *g_b,
@@ -259,7 +267,8 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
        v += (long long)gridDim.x * blockDim.x) {
     const PhaseParams &P = params[phase ? phase[v] : 0];
     for (int al = 0; al < nslip_max; ++al) {
-      const double g = (P.kind == PHASE_EVP && al < P.nslip) ? P.g0 : 0.0;
+      const double g = ((P.kind == PHASE_EVP && al < P.nslip) || (P.kind == PHASE_J2 && al == 0))
+                           ? P.g0 : 0.0;
       g_a[al * V + v] = g;
       g_b[al * V + v] = g;
       g_old[al * V + v] = g;
@@ -277,6 +286,14 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
   for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < V;
        v += (long long)gridDim.x * blockDim.x) {
     const PhaseParams &P = params[phase ? phase[v] : 0];
+    if (P.kind == PHASE_J2) {
+      // isotropic: the unrotated stiffness (isotropic_elastic_plastic.py:55-59)
+#pragma unroll
+      for (int a = 0; a < 6; ++a)
+#pragma unroll
+        for (int b = a; b < 6; ++b) kvox[sym_idx(a, b) * V + v] = (T)P.C[a * 6 + b];
+      continue;
+    }
     const double *Rm = rm_tab + (long long)orient[v] * 36;
     double CR[36];
 #pragma unroll

@@ -96,8 +96,9 @@ struct ssfft_handle {
   PhaseParams hparams[SSFFT_MAX_PHASES];
   bool phase_set[SSFFT_MAX_PHASES];
   PhaseParams *dparams;
-  bool any_evp;
-  int nslip_max;
+  bool any_evp;   // a phase with plastic state (crystal EVP or J2): voxel tangents, state buffers
+  bool any_j2;
+  int nslip_max;  // planes of the slip-state buffers (J2 uses plane 0 for the yield stress)
   // EVP state
   double *g_buf[2];
   int g_cur;
@@ -560,7 +561,7 @@ template <typename T> static int run_minres(ssfft_handle *h, long long *iters, T
 // with the next norms() read-back (no synchronisation here).
 template <typename T>
 static int constitutive(ssfft_handle *h, double dt) {
-  CK(cudaMemsetAsync(h->citers, 0, 2 * sizeof(int), h->stream));
+  CK(cudaMemsetAsync(h->citers, 0, 4 * sizeof(int), h->stream));
   ConstArgs<T> a{};
   a.V = h->V;
   a.eps = (const T *)h->eps;
@@ -590,6 +591,13 @@ static int constitutive(ssfft_handle *h, double dt) {
   a.dt = dt;
   a.max_iters = h->citers;
   a.failed = h->cfail;
+  a.j2 = h->citers + 2;
+  if (h->any_j2) {
+    const int nb = std::max(1, std::min(div_up(h->V, SSFFT_THREADS), 148 * 8));
+    j2_count_kernel<T><<<nb, SSFFT_THREADS, 0, h->stream>>>(a, h->citers + 2);
+    h->launches += 1;
+    CK(cudaGetLastError());
+  }
   const int blocks = std::max(1, std::min(div_up(h->V, CONST_THREADS), 148 * 16));
   constitutive_kernel<T><<<blocks, CONST_THREADS, constitutive_smem_bytes(a.n_params),
                            h->stream>>>(a);
@@ -1021,6 +1029,36 @@ extern "C" int ssfft_set_phase_evp(ssfft_handle *h, int phase, const double stif
   return 0;
 }
 
+extern "C" int ssfft_set_phase_j2(ssfft_handle *h, int phase, double modulus,
+                                  double shear_modulus, double yield_stress, int hardening,
+                                  const double *hardening_props, int n_props) {
+  CKR(check_phase(h, phase));
+  if (hardening < 0 || hardening > 3) return fail(SSFFT_E_INVALID, "unknown hardening law");
+  if (n_props < 0 || n_props > 4) return fail(SSFFT_E_INVALID, "at most 4 hardening properties");
+  if (n_props > 0 && !hardening_props) return fail(SSFFT_E_INVALID, "null hardening properties");
+  const double E = modulus, G = shear_modulus;
+  if (!(G > 0.0) || !(E > 0.0) || 3.0 * G - E == 0.0)
+    return fail(SSFFT_E_INVALID, "J2 moduli must be positive with 3G != E");
+  PhaseParams &P = h->hparams[phase];
+  memset(&P, 0, sizeof(P));
+  P.kind = PHASE_J2;
+  P.nslip = 1;
+  P.hardening = hardening;
+  // Order4SymmetricTensor.from_isotropic_constants (tensor.py:1453-1467), Mandel
+  const double L = G * (E - 2.0 * G) / (3.0 * G - E);
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) P.C[i * 6 + j] = (i == j) ? L + 2.0 * G : L;
+  for (int i = 3; i < 6; ++i) P.C[i * 6 + i] = 2.0 * G;
+  P.shear = G;
+  P.bulk = G * E / (3.0 * (3.0 * G - E));  // isotropic_elastic_plastic.py:28-30
+  P.g0 = yield_stress;
+  P.latent = 1.0;
+  for (int k = 0; k < n_props; ++k) P.props[k] = hardening_props[k];
+  P.E_ref = E;
+  h->phase_set[phase] = true;
+  return 0;
+}
+
 template <typename T> static void build_ktab(const ssfft_handle *h, const std::vector<double> &Rm,
                                              const std::vector<int> &gid_orient,
                                              const std::vector<int> &gid_phase,
@@ -1124,12 +1162,19 @@ extern "C" int ssfft_set_microstructure(ssfft_handle *h, int n_orient, const dou
     max_phase = std::max(max_phase, p);
   }
   h->any_evp = false;
+  h->any_j2 = false;
   h->nslip_max = 0;
-  for (int p = 0; p < SSFFT_MAX_PHASES; ++p)
-    if (h->phase_set[p] && h->hparams[p].kind == PHASE_EVP) {
+  for (int p = 0; p < SSFFT_MAX_PHASES; ++p) {
+    if (!h->phase_set[p]) continue;
+    if (h->hparams[p].kind == PHASE_EVP) {
       h->any_evp = true;
       h->nslip_max = std::max(h->nslip_max, h->hparams[p].nslip);
+    } else if (h->hparams[p].kind == PHASE_J2) {
+      h->any_evp = true;
+      h->any_j2 = true;
+      h->nslip_max = std::max(h->nslip_max, 1);
     }
+  }
   // a handle may be rebound to a new microstructure (serving reuses handles): buffers of
   // the previous binding are kept when large enough, and the captured Krylov launches,
   // which carry their addresses, are dropped
@@ -1378,7 +1423,9 @@ extern "C" int ssfft_get_field(ssfft_handle *h, int field, double *dst, int to_h
     case SSFFT_FIELD_SLIP_RESISTANCES:
     case SSFFT_FIELD_SLIP_SHEAR_STRAINS:
     case SSFFT_FIELD_PLASTIC_STRAINS:
-      if (!h->any_evp) return fail(SSFFT_E_INVALID, "no crystal-plasticity phase in this solve");
+    case SSFFT_FIELD_YIELD_STRESSES:
+    case SSFFT_FIELD_EQ_PLASTIC_STRAINS:
+      if (!h->any_evp) return fail(SSFFT_E_INVALID, "no plastic phase in this solve");
       is_double = true;
       if (field == SSFFT_FIELD_SLIP_RESISTANCES) {
         src = h->g_buf[h->g_cur];
@@ -1386,6 +1433,12 @@ extern "C" int ssfft_get_field(ssfft_handle *h, int field, double *dst, int to_h
       } else if (field == SSFFT_FIELD_SLIP_SHEAR_STRAINS) {
         src = h->gam_trial;
         width = h->nslip_max;
+      } else if (field == SSFFT_FIELD_YIELD_STRESSES) {
+        src = h->g_buf[h->g_cur];  // plane 0
+        width = 1;
+      } else if (field == SSFFT_FIELD_EQ_PLASTIC_STRAINS) {
+        src = h->Gam_trial;
+        width = 1;
       }
       break;
     default: return fail(SSFFT_E_INVALID, "unknown field id");
@@ -1397,8 +1450,8 @@ extern "C" int ssfft_get_field(ssfft_handle *h, int field, double *dst, int to_h
   }
   const int eb = std::max(1, std::min(div_up(V * width, SSFFT_THREADS), 148 * 16));
   if (field == SSFFT_FIELD_PLASTIC_STRAINS) {
-    plastic_to_specimen_kernel<<<eb, SSFFT_THREADS, 0, h->stream>>>(V, h->ep_old, h->orient,
-                                                                     h->rm_tab, ddst);
+    plastic_to_specimen_kernel<<<eb, SSFFT_THREADS, 0, h->stream>>>(
+        V, h->ep_old, h->orient, h->rm_tab, phase_ptr(h), h->dparams, ddst);
   } else if (is_double || h->fp64) {
     to_point_major_kernel<double><<<eb, SSFFT_THREADS, 0, h->stream>>>(V, width,
                                                                        (const double *)src, ddst);

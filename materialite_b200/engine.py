@@ -19,9 +19,11 @@ from . import _native as nat
 
 @dataclass
 class PhaseSpec:
-    """One constitutive phase: ``kind`` is "elastic" or "evp"; stiffness is a 6x6 Mandel
-    matrix.  EVP phases carry Mandel Schmid tensors (S,6) and the parameters of
-    ElasticViscoplastic (elastic_viscoplastic.py:21-50)."""
+    """One constitutive phase: ``kind`` is "elastic", "evp" or "j2"; stiffness is a 6x6
+    Mandel matrix.  EVP phases carry Mandel Schmid tensors (S,6) and the parameters of
+    ElasticViscoplastic (elastic_viscoplastic.py:21-50); J2 phases the parameters of
+    IsotropicElasticPlastic (isotropic_elastic_plastic.py:18-53): ``modulus``,
+    ``shear_modulus`` and the initial yield stress in ``slip_resistance``."""
     kind: str
     stiffness: np.ndarray
     schmid: Optional[np.ndarray] = None
@@ -31,6 +33,8 @@ class PhaseSpec:
     hardening: str = "perfect_plasticity"
     hardening_props: tuple = ()
     latent_ratio: float = 1.0
+    modulus: float = 0.0
+    shear_modulus: float = 0.0
 
 
 def hardening_props_vector(kind, props):
@@ -81,6 +85,7 @@ class SolverHandle:
         nat.check(self.lib.ssfft_create(ctypes.byref(cfg), ctypes.byref(h)))
         self.h = h
         self.nslip = 0
+        self.has_j2 = False
         self.phases = []
 
     def close(self):
@@ -112,6 +117,15 @@ class SolverHandle:
                     float(p.slip_resistance), nat.HARDENING_IDS[p.hardening],
                     nat.as_double_ptr(props), nprops, float(p.latent_ratio)))
                 self.nslip = max(self.nslip, P.shape[0])
+            elif p.kind == "j2":
+                pv = list(hardening_props_vector(p.hardening, p.hardening_props))
+                props = np.ascontiguousarray(pv + [0.0], dtype=np.float64)
+                nat.check(self.lib.ssfft_set_phase_j2(
+                    self.h, i, float(p.modulus), float(p.shear_modulus),
+                    float(p.slip_resistance), nat.HARDENING_IDS[p.hardening],
+                    nat.as_double_ptr(props), len(pv)))
+                self.nslip = max(self.nslip, 1)
+                self.has_j2 = True
             else:
                 raise ValueError(f"unknown phase kind {p.kind}")
 
@@ -155,7 +169,12 @@ class SolverHandle:
         nat.check(self.lib.ssfft_scale_fluctuation(self.h, float(f)))
 
     def field(self, name):
-        width = self.nslip if name in ("slip_resistances", "slip_system_shear_strains") else 6
+        if name in ("slip_resistances", "slip_system_shear_strains"):
+            width = self.nslip
+        elif name in ("yield_stresses", "eq_plastic_strains"):
+            width = 1
+        else:
+            width = 6
         out = np.empty((self.V, width), dtype=np.float64)
         nat.check(self.lib.ssfft_get_field(self.h, nat.FIELD_IDS[name], nat.as_double_ptr(out), 1))
         return out

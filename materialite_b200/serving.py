@@ -93,6 +93,9 @@ class RVERequest:
 
 
 def _phase_struct(p):
+    if p.kind not in ("elastic", "evp"):
+        raise ValueError(f"serving requests take elastic and evp phases, not {p.kind!r}; "
+                         "solve J2 phases through SmallStrainFFT or SolverHandle")
     s = SsfftPhase()
     s.kind = 0 if p.kind == "elastic" else 1
     C = np.asarray(p.stiffness, dtype=np.float64).ravel()

@@ -39,6 +39,15 @@ class Model:
         return material
 
 
+# Which phase kinds carry each state variable (the constitutive models'
+# available_state_variables).
+STATE_VARIABLE_KINDS = {
+    "slip_resistances": ("evp",), "slip_system_shear_strains": ("evp",),
+    "plastic_strains": ("evp", "j2"), "yield_stresses": ("j2",),
+    "eq_plastic_strains": ("j2",),
+}
+
+
 class SmallStrainFFT(Model):
     def __init__(self, load_schedule, end_time=1, initial_time_increment=None,
                  max_time_increment=None, min_time_increment=1.0e-9, start_time=0.0,
@@ -100,8 +109,9 @@ class SmallStrainFFT(Model):
         try:
             handle.set_phases(specs)
             handle.set_microstructure(table, index, phase_of_point)
-            evp_vars = {"slip_resistances", "plastic_strains", "slip_system_shear_strains"}
-            device_vars = [v for v in (output_variables or []) if v in evp_vars and handle.nslip]
+            device_vars = [v for v in (output_variables or [])
+                           if v in STATE_VARIABLE_KINDS and handle.nslip]
+            phase_kinds = [sp.kind for sp in specs]
             comps = lambda f: (lambda t, dt: np.asarray(f(t, dt).components, dtype=float))
             stats = SolveStats()
             nslip = handle.nslip
@@ -110,7 +120,7 @@ class SmallStrainFFT(Model):
 
             def hook(history, h, variables):
                 outs = self._outputs(h, variables, device_vars, V, nslip, phase_of_point,
-                                     phase_slips)
+                                     phase_slips, phase_kinds)
                 outs["stress"] = Order2SymmetricTensor(h.field("stress"), "p")
                 outs["strain"] = Order2SymmetricTensor(h.field("strain"), "p")
                 if postprocessor is not None:
@@ -127,7 +137,7 @@ class SmallStrainFFT(Model):
                                    output_variables=output_variables, stats=stats,
                                    outputs_hook=hook)
             final_outs = self._outputs(handle, output_variables, device_vars, V, nslip,
-                                       phase_of_point, phase_slips)
+                                       phase_of_point, phase_slips, phase_kinds)
             final_outs["stress"] = Order2SymmetricTensor(final["stress"], "p")
             final_outs["strain"] = Order2SymmetricTensor(final["strain"], "p")
             self.last_stats = stats
@@ -148,19 +158,31 @@ class SmallStrainFFT(Model):
         return new_material
 
     @staticmethod
-    def _outputs(handle, variables, device_vars, V, nslip, phase_of_point, phase_slips):
+    def _outputs(handle, variables, device_vars, V, nslip, phase_of_point, phase_slips,
+                 phase_kinds):
         """generate_outputs of the constitutive models (elastic_viscoplastic.py:278-285,
-        multiphase.py:63-95): state variables of EVP phases, None for variables a
-        single-phase model does not have, zeros where a phase lacks them."""
+        isotropic_elastic_plastic.py:177-183, multiphase.py:63-95): state variables of the
+        plastic phases, None for variables a single-phase model does not have, zeros
+        where a phase lacks them."""
         outs = {}
         for v in variables or []:
             if v not in device_vars:
                 outs[v] = None
                 continue
             data = handle.field(v)
+            kinds = STATE_VARIABLE_KINDS[v]
+            if phase_of_point is not None:
+                lacks = np.array([k not in kinds for k in phase_kinds])[phase_of_point]
+                data[lacks] = 0.0
+            elif phase_kinds[0] not in kinds:
+                outs[v] = None
+                continue
             if v == "plastic_strains":
                 outs[v] = Order2SymmetricTensor(data, "p")
+            elif v in ("yield_stresses", "eq_plastic_strains"):
+                outs[v] = Scalar(data[:, 0], "p")
             else:
-                width = max(phase_slips) if phase_slips else nslip
+                evp_slips = [n for n, k in zip(phase_slips, phase_kinds) if k == "evp"]
+                width = max(evp_slips) if evp_slips else nslip
                 outs[v] = Scalar(data[:, :width], "ps")
         return outs

@@ -59,7 +59,7 @@ def cubic_stiffness(C11, C12, C44):
 
 
 def isotropic_stiffness(E, G):
-    """Order4SymmetricTensor.from_isotropic_constants (materialite/tensor.py:1436-1451)."""
+    """Order4SymmetricTensor.from_isotropic_constants (materialite/tensor.py:1453-1467)."""
     L = G * (E - 2 * G) / (3 * G - E)
     V = np.zeros((6, 6))
     V[:3, :3] = L
@@ -263,6 +263,109 @@ class EVPOracle:
         return {"slip_resistances": self.g.copy(),
                 "plastic_strains": self.ep_spec.copy(),
                 "slip_system_shear_strains": self.gam.copy()}
+
+
+def hardening_scalar(kind, props, eq_old, y_old, rate, dt):
+    """The hardening laws called with one scalar rate per point, as IsotropicElasticPlastic
+    calls them (isotropic_elastic_plastic.py:125-131): the increment is dt * |rate|
+    (hardening_laws.py:35-38, the ValueError branch for a Scalar)."""
+    inc = dt * np.abs(rate)
+    if kind == "perfect_plasticity":
+        return y_old.copy()
+    if kind == "linear":
+        return y_old + props["hardening_rate"] * inc
+    if kind == "voce":
+        th0, th1, tau1 = props["theta_0"], props["theta_1"], props["tau_1"]
+        ratio = abs(th0 / tau1)
+        e_i = np.exp(-ratio * eq_old)
+        e_c = np.exp(-ratio * inc)
+        return (y_old + th1 * inc - (ratio * tau1 - th1) / ratio * e_i * (e_c - 1)
+                - th1 / ratio * e_i * (e_c * (1 + ratio * (eq_old + inc)) - 1 - ratio * eq_old))
+    if kind == "armstrong_frederick":
+        h, r = props["direct_hardening"], props["dynamic_recovery"]
+        return y_old + (h - r * y_old) * inc / (1 + r * inc)
+    raise ValueError(f"unknown hardening law {kind}")
+
+
+MANDEL_IDENTITY = np.array([1.0, 1.0, 1.0, 0.0, 0.0, 0.0])
+
+
+class J2Oracle:
+    """IsotropicElasticPlastic: small-strain J2 plasticity with radial return
+    (materialite/models/small_strain_fft/isotropic_elastic_plastic.py:17-183).  The
+    return-mapping loop is the reference's: a fixed-point update of the equivalent plastic
+    strain increment with the constant inverse Jacobian -1/(3G), the residual clipped at
+    zero, repeated for every point until every point has converged (:106-138)."""
+    TOLERANCE = 1.0e-7
+    MAX_ITERATIONS = 100
+
+    def __init__(self, E, G, yield_stress, hardening_kind, hardening_props):
+        self.E, self.G = float(E), float(G)
+        self.Kb = G * E / (3 * (3 * G - E))                              # :28-30
+        self.C = isotropic_stiffness(E, G)
+        self.y0 = float(yield_stress)
+        self.kind, self.props = hardening_kind, hardening_props
+
+    def initialize(self, R):                                           # :55-69
+        V = len(R)
+        self.K = np.tile(self.C, (V, 1, 1))
+        self.ep_old = np.zeros((V, 6))
+        self.eq_old = np.zeros(V)
+        self.y_old = np.full(V, self.y0)
+        self.ep, self.eq, self.y = self.ep_old.copy(), self.eq_old.copy(), self.y_old.copy()
+        return self.K
+
+    def calculate_stress_and_tangent(self, strain, guess, dt):         # :71-164
+        G = self.G
+        ee = strain - self.ep_old
+        tr = ee[:, 0] + ee[:, 1] + ee[:, 2]
+        dev = ee - (1 / 3 * tr)[:, None] * MANDEL_IDENTITY
+        s = 2.0 * G * dev
+        mean = self.Kb * tr
+        q = np.sqrt(1.5) * np.sqrt(np.einsum("pn,pn->p", s, s))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            ratio_s = s / q[:, None]
+        jinv = -1.0 / (3.0 * G)
+        elastic = q <= self.y_old
+        if np.all(elastic):                                            # :94-99
+            return s + mean[:, None] * MANDEL_IDENTITY, self.K, 1
+        dp = np.zeros_like(q)
+        y = self.y_old.copy()
+        it = 0
+        while True:
+            it += 1
+            r = q - 3.0 * G * dp - y
+            r[r <= 0.0] = 0.0
+            prev = dp.copy()
+            dp = dp - jinv * r
+            y = hardening_scalar(self.kind, self.props, self.eq_old, self.y_old, dp / dt, dt)
+            if np.all(np.abs(dp - prev) < self.TOLERANCE):
+                break
+            if it == self.MAX_ITERATIONS:
+                return None, None, 0
+        with np.errstate(invalid="ignore"):
+            self.ep = self.ep_old + 1.5 * ratio_s * dp[:, None]
+        self.eq = self.eq_old + dp
+        self.y = y
+        with np.errstate(divide="ignore", invalid="ignore"):
+            ratio = 3.0 * G / q
+            stress = (1.0 - ratio * dp)[:, None] * s + mean[:, None] * MANDEL_IDENTITY
+            dev_id = np.eye(6) - np.outer(MANDEL_IDENTITY, MANDEL_IDENTITY) / 3.0
+            t1 = 2.0 * G * ratio * dp
+            t2 = ratio**2 * (dp / q - 1 / (3 * G))
+            K = (self.C[None] - t1[:, None, None] * dev_id[None]
+                 + t2[:, None, None] * np.einsum("pm,pn->pmn", s, s))
+        K[elastic] = self.C
+        return stress, K, it
+
+    def update_state_variables(self):                                  # :166-175
+        self.ep_old = self.ep.copy()
+        self.eq_old = self.eq.copy()
+        self.y_old = self.y.copy()
+
+    def outputs(self):
+        return {"yield_stresses": self.y.copy(), "plastic_strains": self.ep.copy(),
+                "eq_plastic_strains": self.eq.copy()}
 
 
 def latent_hardening(g_old, g_iso, gdot, q):

@@ -25,8 +25,8 @@ import pandas as pd  # noqa: E402
 from materialite import (Material, Order2SymmetricTensor, Order4SymmetricTensor,  # noqa: E402
                          Orientation, SlipSystem, Sphere)
 from materialite.models.small_strain_fft import (Elastic, ElasticViscoplastic,  # noqa: E402
-                                                 LoadSchedule, SmallStrainFFT,
-                                                 armstrong_frederick, linear,
+                                                 IsotropicElasticPlastic, LoadSchedule,
+                                                 SmallStrainFFT, armstrong_frederick, linear,
                                                  perfect_plasticity, voce)
 
 from materialite_b200.microstructure import quaternion_random_rotations  # noqa: E402
@@ -194,6 +194,39 @@ def config5_two_phase_small():
          stress=out.extract("stress").components, strain=out.extract("strain").components)
 
 
+def j2_cases():
+    """IsotropicElasticPlastic on heterogeneous microstructures: 8^3 on a 3x3x3 box, 10
+    Voronoi grains (seed 1), each grain phase 0 or 1.  'j2two': phase 0 linear hardening
+    (yield 150, rate 1000), phase 1 Voce (yield 120, 30/10000/100); 'j2incl': phase 0 J2
+    linear, phase 1 cubic elastic inclusions (C11/C12/C44 = 250e3/150e3/120e3).  Uniaxial
+    z at rate 1, dt 1e-4, 15 steps, with the J2 state fields."""
+    rng = np.random.default_rng(1)
+    m = (Material(dimensions=[8, 8, 8], sizes=[3, 3, 3])
+         .create_voronoi(num_regions=10, label="grain", rng=rng)
+         .assign_random_orientations(region_label="grain", rng=rng))
+    grains = m.extract("grain")
+    phase_of_grain = np.array([0, 1, 0, 0, 1, 0, 1, 0, 0, 1])
+    phase = phase_of_grain[grains]
+    m = m.create_fields({"phase": phase})
+    R = m.extract("orientation").rotation_matrix
+    ls = LoadSchedule.from_constant_uniaxial_strain_rate(direction="z")
+    j2lin = IsotropicElasticPlastic(150000.0, 60000.0, 150.0, linear, {"hardening_rate": 1000.0})
+    j2voce = IsotropicElasticPlastic(150000.0, 60000.0, 120.0, voce,
+                                     {"tau_1": 30.0, "theta_0": 10000.0, "theta_1": 100.0})
+    incl = Elastic(Order4SymmetricTensor.from_cubic_constants(250e3, 150e3, 120e3))
+    for tag, models in [("j2two8", [j2lin, j2voce]), ("j2incl8", [j2lin, incl])]:
+        mm = m.create_regional_fields("phase", pd.DataFrame({"phase": [0, 1],
+                                                             "constitutive_model": models}))
+        model = SmallStrainFFT(load_schedule=ls, end_time=15e-4, initial_time_increment=1e-4)
+        out = model(mm, phase_label="phase", global_tolerance=1e-7,
+                    output_variables=["yield_stresses", "plastic_strains", "eq_plastic_strains"])
+        save(tag, rotations=R, phase=phase, stress=out.extract("stress").components,
+             strain=out.extract("strain").components,
+             yield_stresses=np.asarray(out.extract("yield_stresses").components, dtype=float),
+             plastic_strains=out.extract("plastic_strains").components,
+             eq_plastic_strains=out.extract("eq_plastic_strains").components)
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1:
         for name in sys.argv[1:]:
@@ -204,3 +237,4 @@ if __name__ == "__main__":
     reference_evp_cases()
     config3_evp_small()
     config5_two_phase_small()
+    j2_cases()

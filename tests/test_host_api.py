@@ -147,9 +147,6 @@ def test_smallstrainfft_argument_errors():
         SmallStrainFFT(load_schedule=ls, constitutive_model=el)(mat, phase_label="phase")
     with pytest.raises(ValueError, match="must specify phase label"):
         SmallStrainFFT(load_schedule=ls)(mat)
-    j2 = IsotropicElasticPlastic(150000.0, 60000.0, 150.0, linear, {"hardening_rate": 1000.0})
-    with pytest.raises(NotImplementedError):
-        SmallStrainFFT(load_schedule=ls, constitutive_model=j2)(mat)
     with pytest.raises(ValueError):
         SmallStrainFFT(load_schedule=ls, constitutive_model=el, precision="fp16")
 
@@ -172,3 +169,21 @@ def test_vector_outer_and_norm():
     v = Vector([[3.0, 4.0, 0.0]], "s")
     assert_allclose(v.norm.components, [5.0])
     assert v.outer(v).sym.components.shape == (1, 6)
+
+
+def test_j2_phase_spec_maps_reference_parameters():
+    """IsotropicElasticPlastic(modulus, shear_modulus, yield_stress, law, props)
+    (isotropic_elastic_plastic.py:18-53) becomes a "j2" phase."""
+    j2 = IsotropicElasticPlastic(150000.0, 60000.0, 150.0, voce,
+                                 {"tau_1": 30.0, "theta_0": 10000.0, "theta_1": 100.0})
+    spec = j2.phase_spec()
+    assert spec.kind == "j2" and spec.hardening == "voce"
+    assert spec.modulus == 150000.0 and spec.shear_modulus == 60000.0
+    assert spec.slip_resistance == 150.0
+    assert abs(j2.bulk_modulus - 60000.0 * 150000.0 / (3 * (180000.0 - 150000.0))) < 1e-9
+    assert "eq_plastic_strains" in j2.available_state_variables
+
+    def custom(props, a, b, c, d):
+        return b
+    with pytest.raises(NotImplementedError):
+        IsotropicElasticPlastic(150000.0, 60000.0, 150.0, custom, None).phase_spec()

@@ -186,3 +186,67 @@ def test_hardening_laws_closed_forms():
     v = O.hardening("voce", {"tau_1": tau1, "theta_0": th0, "theta_1": 0.0}, Gam,
                     np.repeat(g0[:, None], 12, 1), gdot, dt)
     assert_allclose(v[:, 0], 150.0 + tau1 * (1 - np.exp(-th0 / tau1 * (Gam + dg))))
+
+
+J2_E, J2_G = 150000.0, 60000.0
+
+
+def j2_model(kind, props, y=150.0):
+    return O.J2Oracle(J2_E, J2_G, y, kind, props)
+
+
+@pytest.mark.parametrize("kind,props,end,expected", [
+    ("perfect_plasticity", None, 15e-4, 150.0),
+    ("linear", {"hardening_rate": 1000.0}, 15e-4, 150.3980086),
+    ("voce", {"tau_1": 30.0, "theta_0": 10000.0, "theta_1": 100.0}, 50e-4, 171.694205),
+])
+def test_j2_known_answers(kind, props, end, expected):
+    """test_isotropic_plasticity.py:30-128: mean stress norms of a uniform 8^3 material."""
+    R = np.tile(np.eye(3), (512, 1, 1))
+    out = O.solve((8, 8, 8), R, j2_model(kind, props), O.LoadOracle.uniaxial(1.0, "z"),
+                  end_time=end, initial_time_increment=1e-4)
+    assert_allclose(np.linalg.norm(out["stress"].mean(axis=0)), expected)
+
+
+def test_j2_multiphase_known_answer():
+    """test_multiphase.py:42-73: two identical J2 phases (a box of phase 1 in phase 0)
+    give the uniform answer 150.3980086 and uniform plastic strains."""
+    R = np.tile(np.eye(3), (512, 1, 1))
+    # points in C order (x, y, z) with z fastest; Box(max_corner=[2,2,2]) on a 3x3x3 box
+    xs, ys, zs = [a.ravel() * 3.0 / 7.0 for a in np.meshgrid(np.arange(8), np.arange(8),
+                                                             np.arange(8), indexing="ij")]
+    in_box = (xs <= 2) & (ys <= 2) & (zs <= 2)
+    idx = [np.nonzero(~in_box)[0], np.nonzero(in_box)[0]]
+    lin = {"hardening_rate": 1000.0}
+    model = O.MultiphaseOracle([j2_model("linear", lin), j2_model("linear", lin)], idx, 512)
+    out = O.solve((8, 8, 8), R, model, O.LoadOracle.uniaxial(1.0, "z"), end_time=15e-4,
+                  initial_time_increment=1e-4)
+    assert_allclose(np.linalg.norm(out["stress"].mean(axis=0)), 150.3980086)
+    eq = out["eq_plastic_strains"]
+    assert_allclose(eq, np.full_like(eq, eq.mean()))
+
+
+def j2_golden_model(g, second):
+    phase = g["phase"]
+    idx = [np.nonzero(phase == 0)[0], np.nonzero(phase == 1)[0]]
+    lin = j2_model("linear", {"hardening_rate": 1000.0})
+    if second == "voce":
+        other = j2_model("voce", {"tau_1": 30.0, "theta_0": 10000.0, "theta_1": 100.0}, 120.0)
+    else:
+        other = O.ElasticOracle(O.cubic_stiffness(250e3, 150e3, 120e3))
+    return O.MultiphaseOracle([lin, other], idx, 512)
+
+
+@pytest.mark.parametrize("tag,second", [("j2two8", "voce"), ("j2incl8", "elastic")])
+def test_j2_golden_fields(tag, second):
+    """Heterogeneous J2 solves against fields written by the reference itself."""
+    g = golden(tag)
+    out = O.solve((8, 8, 8), g["rotations"], j2_golden_model(g, second),
+                  O.LoadOracle.uniaxial(1.0, "z"), end_time=15e-4,
+                  initial_time_increment=1e-4, global_tolerance=1e-7)
+    assert rel(out["stress"], g["stress"]) < 1e-10
+    assert rel(out["strain"], g["strain"]) < 1e-10
+    j2 = g["phase"] == 0
+    assert rel(out["eq_plastic_strains"][j2], g["eq_plastic_strains"][j2]) < 1e-9
+    assert rel(out["plastic_strains"][j2], g["plastic_strains"][j2]) < 1e-9
+    assert rel(out["yield_stresses"][j2], g["yield_stresses"][j2]) < 1e-12
