@@ -82,14 +82,15 @@ __host__ __device__ inline int padded_len(int n) { return n + (n >> 4) + 1; }
 // Line layout in shared memory: line l starts at
 //   (l / lsub) * lstride_hi + (l % lsub) * lstride_lo
 // and its element j sits at start + j * estride.
+// The divisors of nlines and lsub come prepared from the host (a device-side make_fastdiv
+// costs a 64-bit division per thread).
 struct LineLayout {
   int nlines, lsub, lstride_hi, lstride_lo, estride;
   FastDiv nl_div, lsub_div;
-  __device__ LineLayout(int nlines_, int lsub_, int hi, int lo, int es)
-      : nlines(nlines_), lsub(lsub_), lstride_hi(hi), lstride_lo(lo), estride(es) {
-    nl_div = make_fastdiv((uint32_t)nlines_);
-    lsub_div = make_fastdiv((uint32_t)lsub_);
-  }
+  __device__ LineLayout(int nlines_, int lsub_, int hi, int lo, int es, const FastDiv &nld,
+                        const FastDiv &lsd)
+      : nlines(nlines_), lsub(lsub_), lstride_hi(hi), lstride_lo(lo), estride(es),
+        nl_div(nld), lsub_div(lsd) {}
   __device__ __forceinline__ int start(int l) const {
     const int g = (int)fdiv((uint32_t)l, lsub_div);
     return g * lstride_hi + (l - g * lsub) * lstride_lo;

@@ -150,6 +150,7 @@ extern "C" int ssfft_apply_projection_noalloc(const int32_t n[3], const double s
   while (g.ky > 1 && smem_y_bytes<double>(g.ky, ny) > 96 * 1024) g.ky /= 2;
   g.kx = std::min(hz, 8);
   while (g.kx > 1 && smem_x_bytes<double>(g.kx, nx) > 100 * 1024) g.kx /= 2;
+  grid_divisors(g);
   const size_t sz = smem_z_bytes<double>(g.lz, nz);
   const size_t sy = smem_y_bytes<double>(g.ky, ny);
   const size_t sx = smem_x_bytes<double>(g.kx, nx);

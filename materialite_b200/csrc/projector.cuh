@@ -33,7 +33,40 @@ template <typename T> struct Grid {
   int lz;                          // (x,y) lines per z-pass block
   int ky;                          // kz columns per y-pass block
   int kx;                          // kz columns per x-pass block
+  // Divisors of the index arithmetic, prepared on the host (grid_divisors): [0] for a full
+  // tile, [1] for the last, partial one along that axis.
+  FastDiv fd_nz, fd_hz, fd_ny, fd_2hz, fd_plane;  // plane kernels: nz, hz, ny, 2 hz, ny hz
+  FastDiv fd_z3[2], fd_znh[2], fd_znz[2];        // z passes: 3 nl, nl hz, nl nz
+  FastDiv fd_ky[2];                              // y passes: nk
+  FastDiv fd_kx[2], fd_x6k[2], fd_xslab[2];      // x pass: nk, 6 nk, nx nk
 };
+
+// Fill the divisor table of a grid whose sizes and tiles (lz, ky, kx) are set.
+template <typename T> inline void grid_divisors(Grid<T> &g) {
+  const long long lines = (long long)g.nx * g.ny;
+  const int nzb = (int)((lines + g.lz - 1) / g.lz);
+  const int lzt = (int)(lines - (long long)(nzb - 1) * g.lz);
+  const int kyt = g.hz - ((g.hz + g.ky - 1) / g.ky - 1) * g.ky;
+  const int kxt = g.hz - ((g.hz + g.kx - 1) / g.kx - 1) * g.kx;
+  auto fd = [](long long d) { return make_fastdiv((uint32_t)d); };
+  g.fd_nz = fd(g.nz);
+  g.fd_hz = fd(g.hz);
+  g.fd_ny = fd(g.ny);
+  g.fd_2hz = fd(2 * g.hz);
+  g.fd_plane = fd((long long)g.ny * g.hz);
+  const int nl[2] = {g.lz, lzt}, ky[2] = {g.ky, kyt}, kx[2] = {g.kx, kxt};
+  for (int t = 0; t < 2; ++t) {
+    g.fd_z3[t] = fd(3LL * nl[t]);
+    g.fd_znh[t] = fd((long long)nl[t] * g.hz);
+    g.fd_znz[t] = fd((long long)nl[t] * g.nz);
+    g.fd_ky[t] = fd(ky[t]);
+    g.fd_kx[t] = fd(kx[t]);
+    g.fd_x6k[t] = fd(6LL * kx[t]);
+    g.fd_xslab[t] = fd((long long)g.nx * kx[t]);
+  }
+}
+
+__device__ __forceinline__ int udiv(int n, const FastDiv &f) { return (int)fdiv((uint32_t)n, f); }
 
 // Shared-memory footprint of the passes (elements of cplx<T>).  The z passes hold three
 // paired lines per (x,y) line, padded (sidx<true>); the x pass pads each component slab
@@ -290,6 +323,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
   const long long nlines_all = (long long)g.nx * g.ny;
   const long long line0 = (long long)blockIdx.x * g.lz;
   const int nl = (int)min((long long)g.lz, nlines_all - line0);
+  const int ti = (nl == g.lz) ? 0 : 1;
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *bufB = bufA + zbuf_elems(g.lz, nz);
   cplx<T> *tw = bufB + zbuf_elems(g.lz, nz);
@@ -298,7 +332,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
   if constexpr (PRO >= PRO_TANGENT_TABLE) u = pending_update<T>(a);
   double xx = 0.0;
   for (int e = threadIdx.x; e < nl * nz; e += blockDim.x) {
-    const int l = e / nz, z = e - (e / nz) * nz;
+    const int l = udiv(e, g.fd_nz), z = e - l * nz;
     const long long v = (line0 + l) * nz + z;
     T tau[6];
     if constexpr (PRO >= PRO_TANGENT_TABLE)
@@ -310,13 +344,13 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
       bufA[sidx<true>((p * nl + l) * nz + z)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
   }
   __syncthreads();
-  const LineLayout L(3 * nl, 3 * nl, 0, nz, 1);
+  const LineLayout L(3 * nl, 3 * nl, 0, nz, 1, g.fd_z3[ti], g.fd_z3[ti]);
   cplx<T> *res = smem_fft<T, false, false, true>(bufA, bufB, L, g.pz, tw);
   // split the paired transform: A = (Z_k + conj Z_{-k}) / 2, B = (Z_k - conj Z_{-k}) / 2i
   for (int e = threadIdx.x; e < 3 * nl * hz; e += blockDim.x) {
-    const int p = e / (nl * hz);
+    const int p = udiv(e, g.fd_znh[ti]);
     const int rem = e - p * nl * hz;
-    const int l = rem / hz, k = rem - (rem / hz) * hz;
+    const int l = udiv(rem, g.fd_hz), k = rem - l * hz;
     const cplx<T> Z = res[sidx<true>((p * nl + l) * nz + k)];
     const int km = (k == 0) ? 0 : nz - k;
     const cplx<T> Zm = res[sidx<true>((p * nl + l) * nz + km)];
@@ -341,6 +375,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
   const int ny = g.ny, hz = g.hz;
   const int k0 = blockIdx.x * g.ky;
   const int nk = min(g.ky, hz - k0);
+  const int ti = (nk == g.ky) ? 0 : 1;
   const int x = blockIdx.y, c = blockIdx.z;
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *bufB = bufA + g.ky * ny;
@@ -348,14 +383,14 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
   load_table<T>(tw, g.twy, ny);
   cplx<T> *base = spec + c * g.S + (long long)x * ny * hz + k0;
   for (int e = threadIdx.x; e < ny * nk; e += blockDim.x) {
-    const int y = e / nk, kk = e - (e / nk) * nk;
+    const int y = udiv(e, g.fd_ky[ti]), kk = e - y * nk;
     bufA[y * nk + kk] = base[(long long)y * hz + kk];
   }
   __syncthreads();
-  const LineLayout L(nk, nk, 0, 1, nk);
+  const LineLayout L(nk, nk, 0, 1, nk, g.fd_ky[ti], g.fd_ky[ti]);
   cplx<T> *res = smem_fft<T, INV, true>(bufA, bufB, L, g.py, tw);
   for (int e = threadIdx.x; e < ny * nk; e += blockDim.x) {
-    const int y = e / nk, kk = e - (e / nk) * nk;
+    const int y = udiv(e, g.fd_ky[ti]), kk = e - y * nk;
     base[(long long)y * hz + kk] = res[y * nk + kk];
   }
 }
@@ -415,6 +450,7 @@ __global__ void __launch_bounds__(XPASS_THREADS)
   const int nx = g.nx, ny = g.ny, hz = g.hz;
   const int k0 = blockIdx.x * g.kx;
   const int nk = min(g.kx, hz - k0);
+  const int ti = (nk == g.kx) ? 0 : 1;
   const int y = blockIdx.y;
   const int slab = nx * nk;                      // live elements per component
   const int sst = xslab_elems<T>(nx, g.kx);      // padded slab stride
@@ -423,16 +459,16 @@ __global__ void __launch_bounds__(XPASS_THREADS)
   cplx<T> *tw = bufB + 6 * sst;
   load_table<T>(tw, g.twx, nx);
   for (int e = threadIdx.x; e < 6 * slab; e += blockDim.x) {
-    const int c = e / slab, rem = e - c * slab;
-    const int x = rem / nk, kk = rem - (rem / nk) * nk;
+    const int c = udiv(e, g.fd_xslab[ti]), rem = e - c * slab;
+    const int x = udiv(rem, g.fd_kx[ti]), kk = rem - x * nk;
     bufA[c * sst + x * nk + kk] = spec[c * g.S + ((long long)x * ny + y) * hz + k0 + kk];
   }
   __syncthreads();
-  const LineLayout L(6 * nk, nk, sst, 1, nk);
+  const LineLayout L(6 * nk, nk, sst, 1, nk, g.fd_x6k[ti], g.fd_kx[ti]);
   cplx<T> *res = smem_fft<T, false, true>(bufA, bufB, L, g.px, tw);
   cplx<T> *other = (res == bufA) ? bufB : bufA;
   for (int e = threadIdx.x; e < slab; e += blockDim.x) {
-    const int x = e / nk, kk = e - (e / nk) * nk;
+    const int x = udiv(e, g.fd_kx[ti]), kk = e - x * nk;
     cplx<T> m[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) m[c] = res[c * sst + x * nk + kk];
@@ -443,8 +479,8 @@ __global__ void __launch_bounds__(XPASS_THREADS)
   __syncthreads();
   cplx<T> *out = smem_fft<T, true, true>(res, other, L, g.px, tw);
   for (int e = threadIdx.x; e < 6 * slab; e += blockDim.x) {
-    const int c = e / slab, rem = e - c * slab;
-    const int x = rem / nk, kk = rem - (rem / nk) * nk;
+    const int c = udiv(e, g.fd_xslab[ti]), rem = e - c * slab;
+    const int x = udiv(rem, g.fd_kx[ti]), kk = rem - x * nk;
     spec[c * g.S + ((long long)x * ny + y) * hz + k0 + kk] = out[c * sst + x * nk + kk];
   }
 }
@@ -512,6 +548,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
   const long long nlines_all = (long long)g.nx * g.ny;
   const long long line0 = (long long)blockIdx.x * g.lz;
   const int nl = (int)min((long long)g.lz, nlines_all - line0);
+  const int ti = (nl == g.lz) ? 0 : 1;
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *bufB = bufA + zbuf_elems(g.lz, nz);
   cplx<T> *tw = bufB + zbuf_elems(g.lz, nz);
@@ -537,9 +574,9 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
   }
   // rebuild the full z spectrum of Z = A + iB from the stored half (Hermitian in z)
   for (int e = threadIdx.x; e < 3 * nel; e += blockDim.x) {
-    const int p = e / nel;
+    const int p = udiv(e, g.fd_znz[ti]);
     const int rem = e - p * nel;
-    const int l = rem / nz, k = rem - (rem / nz) * nz;
+    const int l = udiv(rem, g.fd_nz), k = rem - l * nz;
     const bool low = (k < hz);
     const int ks = low ? k : nz - k;
     const long long off = (line0 + l) * hz + ks;
@@ -549,7 +586,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
         low ? mk<T>(A.x - B.y, A.y + B.x) : mk<T>(A.x + B.y, B.x - A.y);
   }
   __syncthreads();
-  const LineLayout L(3 * nl, 3 * nl, 0, nz, 1);
+  const LineLayout L(3 * nl, 3 * nl, 0, nz, 1, g.fd_z3[ti], g.fd_z3[ti]);
   cplx<T> *res = smem_fft<T, true, false, true>(bufA, bufB, L, g.pz, tw);
   double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
   T c1 = 0;
@@ -683,24 +720,24 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     }
   }
   __syncthreads();
-  const LineLayout Lz(ny, ny, 0, nz, 1);
+  const LineLayout Lz(ny, ny, 0, nz, 1, g.fd_ny, g.fd_ny);
   cplx<T> *res = smem_fft<T, false, false, true>(bufA, bufB, Lz, g.pz, twz);
   cplx<T> *oth = (res == bufA) ? bufB : bufA;
   // split the paired transform into the half spectra of components 2p and 2p+1,
   // laid out [c][y][k] for the y transform
   const int plane = ny * hz;
   for (int e = threadIdx.x; e < plane; e += blockDim.x) {
-    const int y = e / hz, k = e - (e / hz) * hz;
+    const int y = udiv(e, g.fd_hz), k = e - y * hz;
     const cplx<T> Z = res[sidx<true>(y * nz + k)];
     const cplx<T> Zm = res[sidx<true>(y * nz + (k == 0 ? 0 : nz - k))];
     oth[e] = mk<T>((T)0.5 * (Z.x + Zm.x), (T)0.5 * (Z.y - Zm.y));
     oth[plane + e] = mk<T>((T)0.5 * (Z.y + Zm.y), (T)0.5 * (Zm.x - Z.x));
   }
   __syncthreads();
-  const LineLayout Ly(2 * hz, hz, plane, 1, hz);
+  const LineLayout Ly(2 * hz, hz, plane, 1, hz, g.fd_2hz, g.fd_hz);
   cplx<T> *out = smem_fft<T, false, true>(oth, res, Ly, g.py, twy);
   for (int e = threadIdx.x; e < 2 * plane; e += blockDim.x) {
-    const int c = e / plane, rem = e - c * plane;
+    const int c = udiv(e, g.fd_plane), rem = e - c * plane;
     spec[(2 * p + c) * g.S + (long long)x * plane + rem] = out[e];
   }
   if constexpr (PRO >= PRO_TANGENT_TABLE) {
@@ -726,16 +763,16 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
   load_table<T>(twz, g.twz, nz);
   const int plane = ny * hz;
   for (int e = threadIdx.x; e < 2 * plane; e += blockDim.x) {
-    const int c = e / plane, rem = e - c * plane;
+    const int c = udiv(e, g.fd_plane), rem = e - c * plane;
     bufA[e] = spec[(2 * p + c) * g.S + (long long)x * plane + rem];
   }
   __syncthreads();
-  const LineLayout Ly(2 * hz, hz, plane, 1, hz);
+  const LineLayout Ly(2 * hz, hz, plane, 1, hz, g.fd_2hz, g.fd_hz);
   cplx<T> *res = smem_fft<T, true, true>(bufA, bufB, Ly, g.py, twy);
   cplx<T> *oth = (res == bufA) ? bufB : bufA;
   // full z lines of Z = A + iB from the stored halves (Hermitian in z)
   for (int e = threadIdx.x; e < ny * nz; e += blockDim.x) {
-    const int y = e / nz, k = e - (e / nz) * nz;
+    const int y = udiv(e, g.fd_nz), k = e - y * nz;
     const bool low = (k < hz);
     const int ks = low ? k : nz - k;
     const cplx<T> A = res[y * hz + ks];
@@ -743,7 +780,7 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     oth[sidx<true>(e)] = low ? mk<T>(A.x - B.y, A.y + B.x) : mk<T>(A.x + B.y, B.x - A.y);
   }
   __syncthreads();
-  const LineLayout Lz(ny, ny, 0, nz, 1);
+  const LineLayout Lz(ny, ny, 0, nz, 1, g.fd_ny, g.fd_ny);
   cplx<T> *fin = smem_fft<T, true, false, true>(oth, res, Lz, g.pz, twz);
   double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
   T c1 = 0;

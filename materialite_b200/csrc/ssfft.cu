@@ -176,6 +176,7 @@ template <typename T> static Grid<T> make_grid(const ssfft_handle *h) {
   g.lz = h->lz;
   g.ky = h->ky;
   g.kx = h->kx;
+  grid_divisors(g);
   return g;
 }
 
