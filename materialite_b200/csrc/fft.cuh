@@ -92,6 +92,7 @@ struct LineLayout {
       : nlines(nlines_), lsub(lsub_), lstride_hi(hi), lstride_lo(lo), estride(es),
         nl_div(nld), lsub_div(lsd) {}
   __device__ __forceinline__ int start(int l) const {
+    if (lsub == nlines) return l * lstride_lo;  // one group (block-uniform branch)
     const int g = (int)fdiv((uint32_t)l, lsub_div);
     return g * lstride_hi + (l - g * lsub) * lstride_lo;
   }
