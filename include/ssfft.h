@@ -258,6 +258,17 @@ double ssfft_server_clock(ssfft_server *s);
 /* Stops accepting work, finishes running and queued requests, joins the threads. */
 int ssfft_server_destroy(ssfft_server *s);
 
+/* Voronoi region of every point of a dims[0] x dims[1] x dims[2] grid (points at
+ * origin + index * spacing, C order with the last axis fastest): the index of the nearest
+ * of num_regions seeds (num_regions x 3 host array), over the 27 periodic images shifted by
+ * period (the material's sizes, spacing * (dims - 1)) when periodic != 0.  Replaces the
+ * cKDTree query of Material.create_voronoi (material.py:337-383, images as
+ * util.py:57-88) and matches it except for exact distance ties.  region_of_point: host
+ * array of V int32.  Allocates and frees its own device buffers on `device`. */
+int ssfft_voronoi(const int32_t dims[3], const double origin[3], const double spacing[3],
+                  const double period[3], const double *seeds, int num_regions, int periodic,
+                  int device, int32_t *region_of_point);
+
 /* Copy a field out as float64 (V x width).  to_host = 1: dst is host memory;
  * 0: dst is device memory of the handle's device. */
 int ssfft_get_field(ssfft_handle *h, int field, double *dst, int to_host);

@@ -37,7 +37,7 @@ FIELD_IDS = {
 EXPORTED_SYMBOLS = [
     "ssfft_last_error", "ssfft_create", "ssfft_destroy", "ssfft_estimate_bytes",
     "ssfft_set_phase_elastic", "ssfft_set_phase_evp", "ssfft_set_phase_j2",
-    "ssfft_set_microstructure",
+    "ssfft_set_microstructure", "ssfft_voronoi",
     "ssfft_reset", "ssfft_step", "ssfft_commit", "ssfft_scale_fluctuation",
     "ssfft_get_field", "ssfft_num_slip", "ssfft_apply_projection",
     "ssfft_apply_projection_device", "ssfft_stats", "ssfft_timer", "ssfft_profile_krylov",
@@ -148,6 +148,8 @@ def load_library():
     lib.ssfft_set_phase_j2.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_double, ctypes.c_int, dp, ctypes.c_int]
     lib.ssfft_set_microstructure.argtypes = [P, ctypes.c_int, dp, ip, ip]
+    lib.ssfft_voronoi.argtypes = [ip, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  ip]
     lib.ssfft_reset.argtypes = [P]
     lib.ssfft_step.argtypes = [P, ctypes.POINTER(SsfftStepIn), ctypes.POINTER(SsfftStepOut)]
     lib.ssfft_commit.argtypes = [P, ctypes.c_double]

@@ -3,7 +3,7 @@
     python -m materialite_b200.csrc.build
 
 Compiles ``ssfft.cu`` (which includes the kernel headers of this directory),
-``noalloc.cu`` and ``server.cu`` with nvcc into ``materialite_b200/libssfft.so``.
+``noalloc.cu``, ``server.cu`` and ``voronoi.cu`` with nvcc into ``materialite_b200/libssfft.so``.
 """
 
 import os
@@ -33,7 +33,7 @@ def build(force=False, verbose=False):
             and os.path.getmtime(out) >= max(os.path.getmtime(s) for s in srcs)):
         return out
     cmd = [nvcc()] + NVCC_FLAGS + ["-o", out] + [os.path.join(HERE, f) for f in
-                                                 ("ssfft.cu", "noalloc.cu", "server.cu")]
+                                                 ("ssfft.cu", "noalloc.cu", "server.cu", "voronoi.cu")]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

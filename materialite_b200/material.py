@@ -176,12 +176,18 @@ class Material:
         return material
 
     # ---- generators -------------------------------------------------------------------
-    def create_voronoi(self, num_regions=10, label="region", rng=None, periodic=False):
-        """material.py:337-383 (seeds, 27 periodic images shifted by ``sizes``)."""
+    def create_voronoi(self, num_regions=10, label="region", rng=None, periodic=False,
+                       device=None):
+        """material.py:337-383 (seeds, 27 periodic images shifted by ``sizes``).  With
+        ``device`` (a CUDA ordinal) the nearest-seed search runs on that GPU."""
         rng = np.random.default_rng() if rng is None else rng
         seeds = ms.voronoi_seeds(num_regions, self.sizes, self.origin, rng)
-        points = np.column_stack([self._fields["x"], self._fields["y"], self._fields["z"]])
-        regions = ms.nearest_region(points, seeds, self.sizes, periodic)
+        if device is not None:
+            regions = ms.nearest_region_device(self.dimensions, seeds, self.sizes, self.origin,
+                                               self.spacing, periodic, device)
+        else:
+            points = np.column_stack([self._fields["x"], self._fields["y"], self._fields["z"]])
+            regions = ms.nearest_region(points, seeds, self.sizes, periodic)
         return self.create_fields({label: regions})
 
     def assign_random_orientations(self, region_label="region", orientation_label="orientation",

@@ -66,6 +66,35 @@ def periodic_voronoi(dimensions, num_regions, rng, origin=(0, 0, 0), spacing=(1,
     return nearest_region(points, seeds, sizes, periodic)
 
 
+def nearest_region_device(dimensions, seeds, sizes, origin=(0, 0, 0), spacing=(1, 1, 1),
+                          periodic=False, device=0):
+    """nearest_region for the points of a regular grid, on the GPU (ssfft_voronoi): the
+    same regions as the tree query, except for exact distance ties between two seeds."""
+    import ctypes
+
+    from . import _native as nat
+    dims = np.asarray(dimensions, dtype=np.int32)
+    seeds = np.ascontiguousarray(seeds, dtype=np.float64).reshape(-1, 3)
+    out = np.empty(int(np.prod(dims.astype(np.int64))), dtype=np.int32)
+    vec = lambda a: (ctypes.c_double * 3)(*[float(x) for x in a])
+    lib = nat.load_library()
+    nat.check(lib.ssfft_voronoi((ctypes.c_int32 * 3)(*[int(d) for d in dims]), vec(origin),
+                                vec(spacing), vec(sizes), nat.as_double_ptr(seeds),
+                                seeds.shape[0], 1 if periodic else 0, int(device),
+                                nat.as_int_ptr(out)))
+    return out.astype(np.int64)
+
+
+def periodic_voronoi_device(dimensions, num_regions, rng, origin=(0, 0, 0), spacing=(1, 1, 1),
+                            periodic=True, device=0):
+    """periodic_voronoi with the nearest-seed search on the GPU: same seeds from ``rng``,
+    same regions."""
+    dims = np.asarray(dimensions, dtype=int)
+    sizes = np.asarray(spacing, float) * (dims - 1)
+    seeds = voronoi_seeds(num_regions, sizes, origin, rng)
+    return nearest_region_device(dims, seeds, sizes, origin, spacing, periodic, device)
+
+
 def euler_to_rotation(euler):
     """Bunge (z1, x2, z3) -> rotation taking specimen to crystal components
     (tensor.py:1855-1896)."""

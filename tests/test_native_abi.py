@@ -109,3 +109,15 @@ def test_ctypes_structs_match_the_header_layout(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_voronoi_rejects_bad_arguments_before_touching_the_gpu():
+    lib = nat.load_library()
+    dims = (ctypes.c_int32 * 3)(4, 4, 4)
+    vec = (ctypes.c_double * 3)(0.0, 0.0, 0.0)
+    seeds = (ctypes.c_double * 3)(0.5, 0.5, 0.5)
+    out = (ctypes.c_int32 * 64)()
+    assert lib.ssfft_voronoi(dims, vec, vec, vec, seeds, 0, 1, 0, out) == -1  # SSFFT_E_INVALID
+    bad = (ctypes.c_int32 * 3)(4, 0, 4)
+    assert lib.ssfft_voronoi(bad, vec, vec, vec, seeds, 1, 1, 0, out) == -1  # SSFFT_E_INVALID
+    assert b"positive" in lib.ssfft_last_error()
