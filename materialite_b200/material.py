@@ -279,6 +279,35 @@ class Material:
             return type(data[0]).from_list(data)
         return data
 
+    def export_to_evpfft(self, orientation_label="orientation", grain_label="grain",
+                         phase_label="phase", output="fields.txt", euler_angles_to_degrees=True):
+        """The EVP-FFT input file (material.py:1035-1091): one line per point, z slowest
+        and x fastest, "e1 e2 e3 x y z grain phase" with Bunge angles to five decimals and
+        1-based indices.  Warns when a dimension is not a power of two."""
+        import warnings
+        dims = self.dimensions
+        if not all(d > 0 and (d & (d - 1)) == 0 for d in dims.tolist()):
+            warnings.warn("Outputting to EVP-FFT with dimensions that are not powers of 2. Use "
+                          "Material.crop_by_range() or Material.crop_by_id_range() if the "
+                          "dimensions must be powers of 2.")
+        o = self.extract(orientation_label)
+        e = o.euler_angles_in_degrees if euler_angles_to_degrees else o.euler_angles
+        e = np.asarray(e).reshape(-1, 3)
+        ids = [np.asarray(self.extract(k)).astype(np.int64) + 1 for k in ("x_id", "y_id", "z_id")]
+        grains = np.asarray(self.extract(grain_label))
+        phases = np.asarray(self.extract(phase_label))
+        order = np.lexsort((ids[0], ids[1], ids[2]))
+
+        def fmt(a):
+            if np.issubdtype(a.dtype, np.floating):
+                return ["%.5f" % x for x in a[order]]
+            return [str(x) for x in a[order].tolist()]
+
+        cols = [fmt(e[:, 0]), fmt(e[:, 1]), fmt(e[:, 2]), fmt(ids[0]), fmt(ids[1]), fmt(ids[2]),
+                fmt(grains), fmt(phases)]
+        with open(output, "w") as f:
+            f.write("".join(" ".join(row) + "\n" for row in zip(*cols)))
+
     def get_region_volume_fractions(self, region_label="region"):
         vals, counts = np.unique(np.asarray(self._fields[region_label]), return_counts=True)
         return dict(zip(vals.tolist(), counts / self.num_points))

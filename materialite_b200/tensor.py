@@ -613,6 +613,30 @@ class Orientation:
         return cls(np.stack([o.rotation_matrix for o in orientations]), "p")
 
     @property
+    def euler_angles(self):
+        """Bunge (z1, x2, z3) angles of the rotation matrices, the inverse of
+        from_euler_angles (tensor.py:1919-1961, after D. Eberly, "Euler Angle Formulas").
+        With R[2,2] = +-1 the rotation is about z alone and is reported as z1 (x2 = 0 or
+        pi, z3 = 0)."""
+        R = np.asarray(self.rotation_matrix, dtype=np.float64)
+        r22 = R[..., 2, 2]
+        default = (r22 < 1.0) & (r22 > -1.0)
+        with np.errstate(invalid="ignore"):
+            z1 = np.arctan2(R[..., 2, 0], -R[..., 2, 1])
+            x2 = np.arccos(r22)
+            z3 = np.arctan2(R[..., 0, 2], R[..., 1, 2])
+        up = r22 >= 1.0
+        z1 = np.where(default, z1, np.where(up, np.arctan2(-R[..., 1, 0], R[..., 0, 0]),
+                                            np.arctan2(R[..., 1, 0], R[..., 0, 0])))
+        x2 = np.where(default, x2, np.where(up, 0.0, np.pi))
+        z3 = np.where(default, z3, 0.0)
+        return np.squeeze(np.stack([z1, x2, z3], axis=-1))
+
+    @property
+    def euler_angles_in_degrees(self):
+        return self.euler_angles * 180.0 / np.pi
+
+    @property
     def rotation_matrix_mandel(self):
         """6x6 Mandel rotation (tensor.py:1668-1700)."""
         R = self.rotation_matrix

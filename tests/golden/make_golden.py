@@ -227,6 +227,48 @@ def j2_cases():
              eq_plastic_strains=out.extract("eq_plastic_strains").components)
 
 
+def wire_formats():
+    """Files written by the reference's own writers (material.py:1035-1091 export_to_evpfft,
+    json_operations.py:102-122 write_to_json), with the inputs that built them: a 4x4x2
+    material (5 Voronoi grains, random orientations, a spherical phase-2 feature) exported
+    for EVP-FFT in degrees and in radians, and a 6x5x4 material with scalar, tensor,
+    vector-valued, orientation and regional fields and a state, written as JSON."""
+    import json
+
+    from materialite import Scalar, write_to_json
+    rng = np.random.default_rng(7)
+    m = (Material(dimensions=[4, 4, 2])
+         .create_voronoi(num_regions=5, label="grain", rng=rng, periodic=True)
+         .assign_random_orientations(region_label="grain", rng=rng)
+         .create_uniform_field("phase", 1)
+         .insert_feature(Sphere(radius=1.2, centroid=[1, 1, 0]), fields={"phase": 2}))
+    for tag, deg in (("degrees", True), ("radians", False)):
+        out = os.path.join(HERE, f"evpfft_4x4x2_{tag}.txt")
+        m.export_to_evpfft(output=out, euler_angles_to_degrees=deg)
+        print(f"wrote {out}")
+    save("evpfft_4x4x2_inputs", grain=m.extract("grain"), phase=m.extract("phase"),
+         rotations=m.extract("orientation").rotation_matrix)
+    rng = np.random.default_rng(12345)
+    V = 6 * 5 * 4
+    test = rng.random(V)
+    arr = rng.random((V, 3))
+    mj = (Material(dimensions=[6, 5, 4], origin=[1, 2, 3], spacing=[3, 2, 1])
+          .create_voronoi(num_regions=6, label="grain", rng=rng)
+          .assign_random_orientations(region_label="grain", rng=rng)
+          .create_fields({"test": test, "scalar_test": Scalar(test * 100),
+                          "array_test": list(arr)})
+          .create_regional_fields("grain", pd.DataFrame({"grain": np.arange(6),
+                                                         "grain_data": np.arange(6) * 0.1})))
+    mj.state = {"1.0": {"stress": 1}, "2.0": {"strain": [1, 2, 3]}}
+    out = os.path.join(HERE, "material_6x5x4.json")
+    write_to_json(mj, out)
+    print(f"wrote {out} ({os.path.getsize(out) / 1024:.0f} KiB)")
+    save("material_6x5x4_inputs", grain=mj.extract("grain"), test=test, array_test=arr,
+         rotations=mj.extract("orientation").rotation_matrix,
+         regional_rotations=mj.extract_regional_field("grain", "orientation").rotation_matrix)
+    json.loads(open(out).read())
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1:
         for name in sys.argv[1:]:
@@ -238,3 +280,4 @@ if __name__ == "__main__":
     config3_evp_small()
     config5_two_phase_small()
     j2_cases()
+    wire_formats()
