@@ -508,7 +508,7 @@ def solve(dims, R, model, load, end_time=1.0, initial_time_increment=None,
           max_time_increment=None, min_time_increment=1.0e-9, start_time=0.0,
           global_tolerance=1.0e-3, strain_correction_tolerance=1.0e-2,
           linear_solver_tolerance=1.0e-5, output_times=None, output_variables=None,
-          stats=None):
+          stats=None, krylov_maxiter=None):
     """Oracle of ``SmallStrainFFT.run`` (small_strain_fft.py:60-264).  ``model`` is an
     Elastic/EVP/Multiphase oracle; returns a dict of final fields, or of per-output-time
     stacks when ``output_times`` is given."""
@@ -571,7 +571,7 @@ def solve(dims, R, model, load, end_time=1.0, initial_time_increment=None,
                 constit_its.append(cit)
             old_eq = max(eq_err, global_tolerance)
             matvec = lambda v: proj(np.einsum("pmn,pn->pm", tangent, v.reshape(V, 6)))
-            x, kits = minres(matvec, b, linear_solver_tolerance)
+            x, kits = minres(matvec, b, linear_solver_tolerance, krylov_maxiter)
             if stats is not None:
                 stats["krylov"].append(kits)
             fluct = x.reshape(V, 6)

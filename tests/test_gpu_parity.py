@@ -102,3 +102,33 @@ def test_evp_voce_reference_case(precision, tol):
     assert abs(mean_norm - 541.043871) / 541.043871 < max(tol, 1e-7)
     assert rel_l2(out["stress"], ref["stress"]) < tol
     h.close()
+
+
+@pytest.mark.parametrize("device_loop", [True, False])
+def test_krylov_iteration_limit_matches_oracle(device_loop, monkeypatch):
+    """max_krylov_iterations = 4 (scipy's maxiter): every MINRES solve stops at the limit
+    (istop 6) with its last update applied, through the device-side Krylov loop and through
+    the host-polled one; the inexact-Newton solve and its iteration counts match the
+    oracle's."""
+    if not device_loop:
+        monkeypatch.setenv("SSFFT_NO_DEVICE_LOOP", "1")
+    dims = (16, 16, 16)
+    R, C = elastic_case(dims, 20, 0)
+    load = O.LoadOracle.uniaxial(1e-3, "x")
+    ost = {}
+    ref = O.solve(dims, R, O.ElasticOracle(C), load, end_time=3.0, initial_time_increment=1.0,
+                  global_tolerance=1e-6, linear_solver_tolerance=1e-8, stats=ost,
+                  krylov_maxiter=4)
+    table, idx = unique_rotations(R)
+    h = SolverHandle(dims, load.mask, "fp64", global_tolerance=1e-6,
+                     linear_solver_tolerance=1e-8, max_krylov_iterations=4)
+    h.set_phases([PhaseSpec("elastic", C)])
+    h.set_microstructure(table, idx)
+    st = SolveStats()
+    out, _ = solve(h, load.dstrain, load.dstress, load.stress, end_time=3.0,
+                   initial_time_increment=1.0, stats=st)
+    h.close()
+    assert max(ost["krylov"]) == 4
+    assert sum(st.newton_iterations) == len(ost["krylov"])
+    assert sum(st.krylov_iterations) == sum(ost["krylov"])
+    assert rel_l2(out["stress"], ref["stress"]) < 1e-9
