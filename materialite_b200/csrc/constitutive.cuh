@@ -65,9 +65,10 @@ template <typename T> struct ConstArgs {
   const int *j2;           // J2: [0] return-mapping iterations of every point, [1] any plastic
 };
 
-__device__ __forceinline__ void cholesky6(const double *M, double *L) {
+__device__ __forceinline__ void cholesky6(const double *M, double *L, double *inv_diag) {
   // M, L packed symmetric (sym_idx); L holds the lower factor L[i][j], i >= j.  L may be
   // M itself: entry (i, j) of M is read only before entry (i, j) of L is written.
+  // inv_diag receives 1 / L[j][j] for the triangular solves.
 #pragma unroll
   for (int j = 0; j < 6; ++j) {
     double d = M[sym_idx(j, j)];
@@ -76,6 +77,7 @@ __device__ __forceinline__ void cholesky6(const double *M, double *L) {
     const double ljj = sqrt(d);
     L[sym_idx(j, j)] = ljj;
     const double inv = 1.0 / ljj;
+    inv_diag[j] = inv;
 #pragma unroll
     for (int i = j + 1; i < 6; ++i) {
       double s = M[sym_idx(i, j)];
@@ -86,21 +88,22 @@ __device__ __forceinline__ void cholesky6(const double *M, double *L) {
   }
 }
 
-__device__ __forceinline__ void chol_solve6(const double *L, const double *b, double *x) {
+__device__ __forceinline__ void chol_solve6(const double *L, const double *inv_diag,
+                                            const double *b, double *x) {
   double y[6];
 #pragma unroll
   for (int i = 0; i < 6; ++i) {
     double s = b[i];
 #pragma unroll
     for (int k = 0; k < i; ++k) s -= L[sym_idx(i, k)] * y[k];
-    y[i] = s / L[sym_idx(i, i)];
+    y[i] = s * inv_diag[i];
   }
 #pragma unroll
   for (int i = 5; i >= 0; --i) {
     double s = y[i];
 #pragma unroll
     for (int k = i + 1; k < 6; ++k) s -= L[sym_idx(k, i)] * x[k];
-    x[i] = s / L[sym_idx(i, i)];
+    x[i] = s * inv_diag[i];
   }
 }
 
@@ -420,7 +423,7 @@ __global__ void __launch_bounds__(CONST_THREADS, 3) constitutive_kernel(ConstArg
     }
     // linear / Voce / perfect with no latent ratio: one increment for all systems
     const bool iso = (P.latent == 1.0) && (P.hardening != HARD_AF);
-    double ep[6], M[21];
+    double ep[6], M[21], idg[6];
     double dgam = 0.0;
     bool conv = false;
     int it = 0;
@@ -469,8 +472,8 @@ __global__ void __launch_bounds__(CONST_THREADS, 3) constitutive_kernel(ConstArg
         for (int j = 0; j < 6; ++j) acc += P.Cinv[i * 6 + j] * sig[j];
         cr[i] = acc;
       }
-      cholesky6(M, M);
-      chol_solve6(M, cr, z);
+      cholesky6(M, M, idg);
+      chol_solve6(M, idg, cr, z);
       double diff = 0.0;
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
@@ -518,7 +521,7 @@ __global__ void __launch_bounds__(CONST_THREADS, 3) constitutive_kernel(ConstArg
       double e[6], col[6];
 #pragma unroll
       for (int i = 0; i < 6; ++i) e[i] = (i == j) ? 1.0 : 0.0;
-      chol_solve6(M, e, col);
+      chol_solve6(M, idg, e, col);
 #pragma unroll
       for (int i = 0; i <= j; ++i) Tc[sym_idx(i, j)] = col[i];
     }
