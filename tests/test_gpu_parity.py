@@ -132,3 +132,42 @@ def test_krylov_iteration_limit_matches_oracle(device_loop, monkeypatch):
     assert sum(st.newton_iterations) == len(ost["krylov"])
     assert sum(st.krylov_iterations) == sum(ost["krylov"])
     assert rel_l2(out["stress"], ref["stress"]) < 1e-9
+
+
+@pytest.mark.parametrize("dims", [(10, 6, 9), (12, 9, 7)])
+@pytest.mark.parametrize("precision,tol_elastic,tol_evp", [("fp64", 1e-12, 1e-6),
+                                                           ("mixed", 1e-6, 1e-5)])
+def test_solves_on_odd_non_cubic_grids(dims, precision, tol_elastic, tol_evp):
+    """Grids with odd and mixed-radix axes (radix 3, 5, 7 stages, partial tiles).  The
+    elastic solve isolates the transforms and the fused MINRES path: FP64 to round-off.
+    Crystal plasticity (rate exponent 20, two load steps past the onset of slip) differs from
+    the oracle by the per-point stopping of the inner Newton against the reference's
+    half-converged subset rule (elastic_viscoplastic.py:116-158), up to ~6e-7 here."""
+    R = voronoi_micro(dims, max(2, int(np.prod(dims)) // 40), 5)
+    C = O.cubic_stiffness(250.0, 150.0, 120.0)
+    n, d = O.octahedral_slip_systems()
+    P = O.schmid_mandel(n, d)
+    props = {"tau_1": 0.2, "theta_0": 1.0, "theta_1": 0.0}
+    load = O.LoadOracle.uniaxial(1e-3, "x")
+    table, idx = unique_rotations(R)
+
+    refe = O.solve(dims, R, O.ElasticOracle(C), load, end_time=2.0, initial_time_increment=1.0,
+                   global_tolerance=1e-6, linear_solver_tolerance=1e-8)
+    h = SolverHandle(dims, load.mask, precision, global_tolerance=1e-6,
+                     linear_solver_tolerance=1e-8)
+    h.set_phases([PhaseSpec("elastic", C)])
+    h.set_microstructure(table, idx)
+    oute, _ = solve(h, load.dstrain, load.dstress, load.stress, end_time=2.0,
+                    initial_time_increment=1.0)
+    h.close()
+    assert rel_l2(oute["stress"], refe["stress"]) < tol_elastic
+
+    ref = O.solve(dims, R, O.EVPOracle(C, P, 1e-3, 20.0, 0.1, "voce", props), load,
+                  end_time=1.2, initial_time_increment=0.6, global_tolerance=1e-6)
+    h = SolverHandle(dims, load.mask, precision, global_tolerance=1e-6)
+    h.set_phases([PhaseSpec("evp", C, P, 1e-3, 20.0, 0.1, "voce", props)])
+    h.set_microstructure(table, idx)
+    out, _ = solve(h, load.dstrain, load.dstress, load.stress, end_time=1.2,
+                   initial_time_increment=0.6)
+    h.close()
+    assert rel_l2(out["stress"], ref["stress"]) < tol_evp
