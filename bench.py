@@ -462,6 +462,32 @@ def serve_mode(args, w):
     replicas.destroy(world)
 
 
+def sweep_mode(args, w):
+    """Arrival-rate sweep of the serving stream on one warm server: the same seeded
+    requests submitted as Poisson arrivals at each rate of ``--rates``; per rate the served
+    solves/s (count / makespan from first arrival to last completion) and the p50/p99/mean
+    latency from submission to completion."""
+    from materialite_b200.serving import RVEServer, latency_stats, request_stream, run_stream
+    count = args.count or 32
+    rates = [float(x) for x in args.rates.split(",")]
+    srv = RVEServer(device=0, max_slots=w["slots"], precision="mixed")
+    run_stream(srv, request_stream(min(count, 8), 0.0, seed=w["seed"]), timeout=1800)
+    out = {"workload": f"serve sweep: {count} requests of the serving stream, "
+                       f"{w['slots']} slots, mixed precision", "rates": []}
+    for rate in rates:
+        reqs = request_stream(count, rate, seed=w["seed"])
+        comps, span = run_stream(srv, reqs, timeout=1800)
+        bad = [c.tag for c in comps if c.status != 0]
+        if bad:
+            raise RuntimeError(f"requests failed: {bad}")
+        lat = latency_stats(comps)
+        out["rates"].append({"rate_per_s": rate, "solves_per_s": count / span,
+                             "makespan_s": span, **lat})
+        print(json.dumps(out["rates"][-1]), flush=True)
+    srv.close()
+    print(json.dumps(out), flush=True)
+
+
 def request_mode(args, w):
     """One request of the serving stream (``--tag``), alone, in the chosen precision:
     the target of per-request kernel profiles."""
@@ -570,12 +596,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--mode", default="bench",
-                    choices=["bench", "kernels", "request", "accuracy"],
+                    choices=["bench", "kernels", "request", "accuracy", "sweep"],
                     help="kernels: one load increment, then the Krylov kernels timed in "
                          "isolation (the target of the ncu captures under profiles/); "
                          "request: one request of the serving stream alone; accuracy: one "
                          "solve of the workload in mixed and in FP64, stress error between")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--rates", default="1,2,4,8,50",
+                    help="sweep: Poisson arrival rates (requests/s)")
     ap.add_argument("--load-steps", type=int, default=0,
                     help="accuracy: solve only the first N load increments of the workload")
     ap.add_argument("--count", type=int, default=0, help="serve: number of requests")
@@ -592,6 +620,9 @@ def main():
         return
     if args.mode == "request":
         request_mode(args, WORKLOADS["serve"])
+        return
+    if args.mode == "sweep":
+        sweep_mode(args, WORKLOADS["serve"])
         return
     if args.workload == "serve" and args.impl == "ours":
         serve_mode(args, w)
