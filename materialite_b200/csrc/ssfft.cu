@@ -239,7 +239,9 @@ static int plan_tiles(ssfft_handle *h) {
   h->lz = (int)std::min<long long>(h->lz, (long long)h->nx * h->ny);
   h->ky = std::min(h->hz, 16);
   while (h->ky > 1 && smem_y_bytes<double>(h->ky, h->ny) > 96 * 1024) h->ky /= 2;
-  h->kx = std::min(h->hz, 8);
+  // kz columns per x-pass block: 8 (64-byte runs of the spectrum per x), 4 on grids of up
+  // to 64 points along x, where 8 would leave about two blocks per SM
+  h->kx = std::min(h->hz, h->nx <= 64 ? 4 : 8);
   while (h->kx > 1 && smem_x_bytes<double>(h->kx, h->nx) > 100 * 1024) h->kx /= 2;
   h->smem_z = smem_z_bytes<double>(h->lz, h->nz);
   h->smem_y = smem_y_bytes<double>(h->ky, h->ny);
