@@ -7,6 +7,7 @@ per-step Newton/Krylov work runs on the GPU inside ``ssfft_step``.
 """
 
 import ctypes
+import logging
 import math
 from collections import defaultdict
 from dataclasses import dataclass, field
@@ -215,6 +216,10 @@ class SolveStats:
     device_seconds: float = 0.0
 
 
+# the reference's logger name (small_strain_fft.py:53)
+_log = logging.getLogger("SmallStrainFFT")
+
+
 def solve(handle, dstrain, dstress, stress, end_time=1.0, initial_time_increment=None,
           max_time_increment=None, min_time_increment=1.0e-9, start_time=0.0,
           output_times=None, output_variables=None, stats=None, outputs_hook=None):
@@ -243,7 +248,15 @@ def solve(handle, dstrain, dstress, stress, end_time=1.0, initial_time_increment
         Sbar = np.asarray(stress(t, dt), dtype=np.float64).reshape(6)
         max_inc = dE[np.argmax(np.abs(dE))]
         reset = max_inc * old_max_inc < 0.0
+        _log.info(f"New increment: time {t} + {dt}")
         out = handle.step(dE, dS, Sbar, dt, summed_vm, step_id, reset)
+        # the Newton loop runs on the device; its outcome is logged once per increment
+        _log.debug(f"global iterations {out.newton_iterations}")
+        _log.debug(f"linear solver iterations: {out.krylov_iterations}")
+        _log.debug(f"equilibrium error: {out.equilibrium_error}")
+        _log.debug(f"scaled strain error: {out.scaled_strain_error}")
+        if not out.converged and not out.constitutive_failed:
+            _log.info("Too many iterations in macroloading loop")
         if stats is not None:
             stats.newton_iterations.append(out.newton_iterations)
             stats.krylov_iterations.append(out.krylov_iterations)
