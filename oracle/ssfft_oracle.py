@@ -115,8 +115,8 @@ def dev_norm(s):
 
 def hardening(kind, props, Gamma_old, g_old, gdot, dt, latent=1.0):
     """Slip resistances after an increment.  ``Gamma_old`` (V,), ``g_old`` and ``gdot``
-    (V, S).  Laws follow hardening_laws.py:18-90; ``latent`` != 1 is this build's
-    extension (no reference counterpart) and is only applied by the caller."""
+    (V, S).  Laws follow hardening_laws.py:18-90; ``latent`` != 1 is a latent-hardening
+    extension with no reference counterpart, applied only by the caller."""
     dgam = dt * np.sum(np.abs(gdot), axis=-1)  # hardening_laws.py:35-38 / 49-52 / 83-86
     if kind == "perfect_plasticity":          # :18-25
         return g_old.copy()
