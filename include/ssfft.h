@@ -297,9 +297,10 @@ int ssfft_apply_projection_device(ssfft_handle *h, const void *in_dev, void *out
  * Its scratch (spectrum and FFT tables) is one file-scope device array of about 13 MB
  * that every GPU loading the library holds until exit; grids are limited to
  * nx*ny*(nz/2+1) <= 135168 (64^3) and 1024 points per axis, larger ones are rejected.
- * The first call on a device (current device) looks up the array's address once; make
- * it before any stream capture.  All calls share the array: calls that overlap on the
- * GPU race.  Calls no cudaMalloc, cudaFree or allocating library routine. */
+ * The first call on a device (current device) looks up the array's address once and
+ * keeps it for the life of the process; make it before any stream capture, and do not
+ * call again on a device after cudaDeviceReset() there.  All calls share the array:
+ * calls that overlap on the GPU race.  Calls no cudaMalloc, cudaFree or allocating library routine. */
 int ssfft_apply_projection_noalloc(const int32_t n[3], const double stress_mask[6],
                                    const double *in_dev, double *out_dev, void *stream);
 

@@ -14,7 +14,10 @@
 //   * at most NOALLOC_MAX_SPEC_POINTS half-spectrum points (nx * ny * (nz/2 + 1)), i.e.
 //     grids up to 64^3, and at most 1024 points per axis; larger grids are rejected;
 //   * the first call on a device looks up the array's device address and sets kernel
-//     attributes (once per device); make that first call before any stream capture;
+//     attributes (once per device, kept for the life of the process); make that first
+//     call before any stream capture.  The cached address belongs to the device's primary
+//     context: after cudaDeviceReset() on that device, do not call this entry point again
+//     in the same process;
 //   * every call shares the one array: calls that overlap on the GPU (for example on two
 //     streams) race and corrupt each other's results.  The spectrum is completely
 //     overwritten by each call, so nothing needs clearing between calls.
@@ -143,7 +146,8 @@ extern "C" int ssfft_apply_projection_noalloc(const int32_t n[3], const double s
   g.tanz = tn + 2 * NOALLOC_MAX_AXIS;
   g.scale = 1.0 / (double)g.V;
   for (int c = 0; c < 6; ++c) g.mask[c] = stress_mask[c];
-  // tiles as in the handle-based path (double-precision transforms)
+  // tiles of the handle-based path's double-precision transforms, except that the x pass
+  // always takes 8 kz columns per block (the handle path takes 4 on axes of up to 64)
   g.lz = nz >= 3 * 2048 ? 1 : std::max(1, std::min(32, 2048 / (3 * nz)));
   g.lz = (int)std::min<long long>(g.lz, (long long)nx * ny);
   g.ky = std::min(hz, 16);

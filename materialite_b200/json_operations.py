@@ -1,3 +1,9 @@
+# Portions of this file restate the interface and the JSON document layout of materialite's
+# materialite/json_operations.py: Copyright 2025 United States Government as represented by the Administrator
+# of the National Aeronautics and Space Administration.  All Rights Reserved.  Licensed
+# under the Apache License, Version 2.0 (http://www.apache.org/licenses/LICENSE-2.0);
+# distributed on an "AS IS" BASIS, WITHOUT WARRANTIES OR CONDITIONS OF ANY KIND.
+
 """JSON persistence of a Material, in the layout of materialite/json_operations.py:23-122,
 so that files move between this package and the reference: a "metadata" entry (origin,
 dimensions, spacing), an optional "state", "regional_fields" by region label, and one

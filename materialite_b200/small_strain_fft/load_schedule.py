@@ -1,3 +1,9 @@
+# Portions of this file restate the interface and the boundary-condition closures of materialite's
+# materialite/models/small_strain_fft/load_schedule.py: Copyright 2025 United States Government as represented by the Administrator
+# of the National Aeronautics and Space Administration.  All Rights Reserved.  Licensed
+# under the Apache License, Version 2.0 (http://www.apache.org/licenses/LICENSE-2.0);
+# distributed on an "AS IS" BASIS, WITHOUT WARRANTIES OR CONDITIONS OF ANY KIND.
+
 """Mixed strain/stress boundary conditions as closures of (t, dt)
 (materialite/models/small_strain_fft/load_schedule.py:17-119)."""
 

@@ -4,8 +4,9 @@
 The reference imports pyvista, h5py, matplotlib and cupy at module level for plotting,
 file import and its GPU process models; none of them is on the SmallStrainFFT path.
 Empty placeholder modules are registered for them before import, which changes no
-arithmetic.  The reference is read from ``MATERIALITE_REFERENCE`` (default
-``/root/reference``) and is never needed on a machine that only runs the GPU tests.
+arithmetic.  The reference checkout is named by the ``MATERIALITE_REFERENCE``
+environment variable (there is no default); it is never needed on a machine that only runs
+the GPU tests.
 """
 
 import os
@@ -18,17 +19,20 @@ _STUBS = ["pyvista", "h5py", "matplotlib", "matplotlib.pyplot", "matplotlib.colo
 
 
 def reference_root():
-    return os.environ.get("MATERIALITE_REFERENCE", "/root/reference")
+    """The reference checkout named by MATERIALITE_REFERENCE, or None when unset."""
+    return os.environ.get("MATERIALITE_REFERENCE") or None
 
 
 def available():
-    return os.path.isfile(os.path.join(reference_root(), "materialite", "__init__.py"))
+    root = reference_root()
+    return root is not None and os.path.isfile(os.path.join(root, "materialite", "__init__.py"))
 
 
 def import_reference():
     """Return the reference ``materialite`` module (raises ImportError if absent)."""
     if not available():
-        raise ImportError("reference materialite checkout not found")
+        raise ImportError("reference materialite checkout not found: set MATERIALITE_REFERENCE "
+                          "to the directory that contains the materialite package")
     for name in _STUBS:
         sys.modules.setdefault(name, types.ModuleType(name))
     root = reference_root()

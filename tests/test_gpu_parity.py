@@ -12,6 +12,17 @@ from materialite_b200.microstructure import (bunge_random_rotations, first_appea
 pytestmark = pytest.mark.gpu
 
 UNIAXIAL_X_MASK = [0, 1, 1, 1, 1, 1]
+# The two projector pipelines of a Krylov iteration: plane-fused z+y passes (grids whose yz
+# plane fits in shared memory) and the five-pass fallback of larger grids, forced here on
+# small grids with SSFFT_NO_PLANE=1 (read when a handle is created).
+PATHS = ["plane", "five_pass"]
+
+
+def use_path(monkeypatch, path):
+    if path == "five_pass":
+        monkeypatch.setenv("SSFFT_NO_PLANE", "1")
+    else:
+        monkeypatch.delenv("SSFFT_NO_PLANE", raising=False)
 
 
 def rel_l2(a, b):
@@ -28,11 +39,13 @@ def voronoi_micro(dims, grains, seed, spacing=(1, 1, 1), periodic=True):
     return R[lut[ids]]
 
 
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("dims", [(4, 4, 4), (3, 4, 5), (6, 5, 8), (16, 16, 16), (12, 9, 7),
                                   (32, 16, 8), (1, 4, 6)])
 @pytest.mark.parametrize("mask", [[0, 0, 0, 0, 0, 0], UNIAXIAL_X_MASK, [1] * 6])
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 3e-6)])
-def test_projection_matches_oracle(dims, mask, precision, tol):
+def test_projection_matches_oracle(dims, mask, precision, tol, path, monkeypatch):
+    use_path(monkeypatch, path)
     V = int(np.prod(dims))
     tau = np.random.default_rng(7).standard_normal((V, 6))
     h = SolverHandle(dims, mask, precision)
@@ -48,10 +61,12 @@ def elastic_case(dims, grains, seed):
     return R, C
 
 
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-5)])
-def test_elastic_voronoi_solve(precision, tol):
+def test_elastic_voronoi_solve(precision, tol, path, monkeypatch):
     """Config-1 physics at 16^3 (20 periodic Voronoi grains, cubic 250/150/120,
     uniaxial x strain rate 1e-3), 4 steps."""
+    use_path(monkeypatch, path)
     dims = (16, 16, 16)
     R, C = elastic_case(dims, 20, 0)
     load = O.LoadOracle.uniaxial(1e-3, "x")
@@ -77,10 +92,12 @@ def evp_voce_phase(C):
     return O.schmid_mandel(n, d)
 
 
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-7), ("mixed", 1e-5)])
-def test_evp_voce_reference_case(precision, tol):
+def test_evp_voce_reference_case(precision, tol, path, monkeypatch):
     """tests/test_elastic_viscoplastic_model.py:147-161 of the reference: 8^3 grid on a
     3x3x3 box, 10 Voronoi grains (seed 0), Voce hardening; mean stress norm 541.043871."""
+    use_path(monkeypatch, path)
     dims = (8, 8, 8)
     R = voronoi_micro(dims, 10, 0, spacing=(3 / 7,) * 3, periodic=False)
     Cv = np.array([[160e3, 90e3, 66e3, 0, 0, 0], [90e3, 160e3, 66e3, 0, 0, 0],
@@ -104,12 +121,14 @@ def test_evp_voce_reference_case(precision, tol):
     h.close()
 
 
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("device_loop", [True, False])
-def test_krylov_iteration_limit_matches_oracle(device_loop, monkeypatch):
+def test_krylov_iteration_limit_matches_oracle(device_loop, path, monkeypatch):
     """max_krylov_iterations = 4 (scipy's maxiter): every MINRES solve stops at the limit
     (istop 6) with its last update applied, through the device-side Krylov loop and through
     the host-polled one; the inexact-Newton solve and its iteration counts match the
     oracle's."""
+    use_path(monkeypatch, path)
     if not device_loop:
         monkeypatch.setenv("SSFFT_NO_DEVICE_LOOP", "1")
     dims = (16, 16, 16)
@@ -134,15 +153,18 @@ def test_krylov_iteration_limit_matches_oracle(device_loop, monkeypatch):
     assert rel_l2(out["stress"], ref["stress"]) < 1e-9
 
 
+@pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("dims", [(10, 6, 9), (12, 9, 7)])
 @pytest.mark.parametrize("precision,tol_elastic,tol_evp", [("fp64", 1e-12, 1e-6),
                                                            ("mixed", 1e-6, 1e-5)])
-def test_solves_on_odd_non_cubic_grids(dims, precision, tol_elastic, tol_evp):
+def test_solves_on_odd_non_cubic_grids(dims, precision, tol_elastic, tol_evp, path,
+                                       monkeypatch):
     """Grids with odd and mixed-radix axes (radix 3, 5, 7 stages, partial tiles).  The
     elastic solve isolates the transforms and the fused MINRES path: FP64 to round-off.
     Crystal plasticity (rate exponent 20, two load steps past the onset of slip) differs from
     the oracle by the per-point stopping of the inner Newton against the reference's
     half-converged subset rule (elastic_viscoplastic.py:116-158), up to ~6e-7 here."""
+    use_path(monkeypatch, path)
     R = voronoi_micro(dims, max(2, int(np.prod(dims)) // 40), 5)
     C = O.cubic_stiffness(250.0, 150.0, 120.0)
     n, d = O.octahedral_slip_systems()
