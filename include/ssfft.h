@@ -199,13 +199,16 @@ int ssfft_solve_constant_rates(ssfft_handle *h, const ssfft_rate_schedule *sched
                                ssfft_solve_out *out);
 
 /* ---- serving ---------------------------------------------------------------------
- * A server keeps up to max_slots RVE solves resident on one GPU, each with its own
- * handle and CUDA stream, driven by its own host thread, so that the work of requests that
- * arrive while others run overlaps on the device (continuous batching at request
- * granularity).  A queued request is admitted when a slot is free and its device memory
- * (ssfft_estimate_bytes) fits both the server's budget and cudaMemGetInfo's free memory.
- * Results do not depend on what else runs: every reduction of a solve is private to its
- * handle and summed in a fixed order. */
+ * A server solves many RVE requests at once on one GPU.  Requests of one class (grid,
+ * precision, elastic or crystal-plasticity tangents, slip-system count, stress rates or
+ * not) share a group of up to max_slots slots; every kernel launch of a group covers all
+ * of its resident requests, whose Newton iterations advance together in rounds run by a
+ * CUDA graph, with the Newton decisions, commits, dt adaptation and cutbacks made on the
+ * device.  A queued request joins its group at the next round boundary when a slot is
+ * free; a slot's device memory (ssfft_estimate_bytes) is allocated on its first use, when
+ * it fits both the server's budget and cudaMemGetInfo's free memory.  Classes run
+ * concurrently.  Results do not depend on what else runs: every reduction of a request is
+ * private to its slot and summed in a fixed order. */
 
 /* One phase of a request (the arguments of ssfft_set_phase_elastic / _evp). */
 typedef struct {
@@ -255,6 +258,8 @@ int ssfft_server_poll(ssfft_server *s, ssfft_completion *out, int max, int *n_ou
 /* Requests submitted but not yet polled (queued + running + finished-unpolled). */
 int ssfft_server_pending(ssfft_server *s);
 double ssfft_server_clock(ssfft_server *s);
+/* Kernels the server's groups have launched so far (graph replays counted per kernel). */
+int ssfft_server_launches(ssfft_server *s, int64_t *kernel_launches);
 /* Stops accepting work, finishes running and queued requests, joins the threads. */
 int ssfft_server_destroy(ssfft_server *s);
 

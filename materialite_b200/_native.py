@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = [
     "ssfft_apply_projection_device", "ssfft_stats", "ssfft_timer", "ssfft_profile_krylov",
     "ssfft_apply_projection_noalloc", "ssfft_solve_constant_rates", "ssfft_set_options",
     "ssfft_server_create", "ssfft_server_submit", "ssfft_server_poll", "ssfft_server_pending",
-    "ssfft_server_clock", "ssfft_server_destroy",
+    "ssfft_server_clock", "ssfft_server_destroy", "ssfft_server_launches",
 ]
 
 

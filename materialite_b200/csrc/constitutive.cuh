@@ -16,7 +16,9 @@
 // the same tolerance of the same Newton iteration.
 #pragma once
 
+#include "../../include/ssfft.h"
 #include "common.cuh"
+#include "slots.cuh"
 
 #define EVP_TOLERANCE 2.0e-5
 #define EVP_MAX_ITERATIONS 60
@@ -175,6 +177,47 @@ __device__ __forceinline__ void load6(const T *f, long long V, long long v, doub
   for (int c = 0; c < 6; ++c) x[c] = (double)f[c * V + v];
 }
 
+// Threads of a constitutive block, and points of one item (four per thread).
+#define CONST_THREADS 128
+#define CONST_POINTS (4 * CONST_THREADS)
+
+__host__ __device__ inline int const_items(long long V) {
+  return (int)((V + CONST_POINTS - 1) / CONST_POINTS);
+}
+
+// The constitutive call of one slot: strain and stress guess in, stress and tangent out,
+// plastic trial state written from the committed one (elastic_viscoplastic.py:91-188).
+template <typename T>
+__device__ __forceinline__ ConstArgs<T> const_args(const SlotDev<T> &S, long long V) {
+  ConstArgs<T> a;
+  a.V = V;
+  a.eps = S.eps;
+  a.guess = S.sig;
+  a.sig = S.sig_next;
+  a.kvox = S.voxel_mode ? S.kvox : nullptr;
+  a.ktab = S.ktab;
+  a.gid = S.gid;
+  a.phase = S.phase;
+  a.orient = S.orient;
+  a.params = S.params;
+  a.n_params = S.n_params;
+  a.rm_tab = S.rm_tab;
+  a.g_in = S.g_in;
+  a.g_out = S.g_out;
+  a.g_old = S.g_old;
+  a.ep_old = S.ep_old;
+  a.ep_trial = S.ep_trial;
+  a.Gam_old = S.Gam_old;
+  a.Gam_trial = S.Gam_trial;
+  a.gam_old = S.gam_old;
+  a.gam_trial = S.gam_trial;
+  a.dt = S.dt;
+  a.max_iters = S.citers;
+  a.failed = S.citers + 1;
+  a.j2 = S.citers + 2;
+  return a;
+}
+
 // ---------------- J2 plasticity (isotropic_elastic_plastic.py:71-164) ----------------
 #define J2_TOLERANCE 1.0e-7
 #define J2_MAX_ITERATIONS 100
@@ -221,8 +264,18 @@ __device__ __forceinline__ double j2_update(const PhaseParams &P, double q, doub
 // with j2[1] = 1 if any point is plastic.  A point that does not converge within
 // J2_MAX_ITERATIONS fails the update (:133-137).
 template <typename T>
-__global__ void __launch_bounds__(SSFFT_THREADS) j2_count_kernel(ConstArgs<T> a, int *j2) {
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    j2_count_kernel(const SlotDev<T> *__restrict__ tab, SlotList list, long long V) {
   __shared__ int blk_n, blk_any, blk_fail;
+  const int per = const_items(V);
+  const int n_items = list_items(list, per);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+  const int kslot = item / per;
+  const int local = item - kslot * per;
+  const SlotDev<T> &S = tab[list.ids[kslot]];
+  const ConstArgs<T> a = const_args<T>(S, V);
+  int *j2 = S.citers + 2;
+  __syncthreads();
   if (threadIdx.x == 0) {
     blk_n = 0;
     blk_any = 0;
@@ -230,9 +283,8 @@ __global__ void __launch_bounds__(SSFFT_THREADS) j2_count_kernel(ConstArgs<T> a,
   }
   __syncthreads();
   int my_n = 0, my_any = 0, my_fail = 0;
-  const long long V = a.V;
-  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < V;
-       v += (long long)gridDim.x * blockDim.x) {
+  const long long v1 = min(V, (long long)(local + 1) * CONST_POINTS);
+  for (long long v = (long long)local * CONST_POINTS + threadIdx.x; v < v1; v += blockDim.x) {
     const PhaseParams &P = a.params[a.phase ? a.phase[v] : 0];
     if (P.kind != PHASE_J2) continue;
     double eps[6], epo[6], s[6], mean, q;
@@ -266,23 +318,25 @@ __global__ void __launch_bounds__(SSFFT_THREADS) j2_count_kernel(ConstArgs<T> a,
     if (blk_any) atomicOr(&j2[1], 1);
     if (blk_fail) atomicOr(a.failed, 1);
   }
+  }
 }
 
 // Threads of a constitutive block, and the shared memory a block holds: the phase table
 // plus per-thread slip arrays (old and current resistances, slip rates) and the two
 // crystal-frame strain vectors, [entry][thread] so that a warp's accesses are contiguous.
-#define CONST_THREADS 128
-inline size_t constitutive_smem_bytes(int n_params) {
-  return (size_t)n_params * sizeof(PhaseParams) +
+inline size_t constitutive_smem_bytes() {
+  return (size_t)SSFFT_MAX_PHASES * sizeof(PhaseParams) +
          (size_t)(3 * MAX_SLIP + 12) * CONST_THREADS * sizeof(double);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(CONST_THREADS, 3) constitutive_kernel(ConstArgs<T> a) {
+__global__ void __launch_bounds__(CONST_THREADS, 3)
+    constitutive_kernel(const SlotDev<T> *__restrict__ tab, SlotList list, long long V) {
   extern __shared__ __align__(16) unsigned char csm[];
   PhaseParams *sp = reinterpret_cast<PhaseParams *>(csm);
   const int tid = threadIdx.x;
-  double *s_gold = reinterpret_cast<double *>(sp + a.n_params) + tid;  // stride CONST_THREADS
+  // per-thread slip arrays after the largest phase table, stride CONST_THREADS
+  double *s_gold = reinterpret_cast<double *>(sp + SSFFT_MAX_PHASES) + tid;
   double *s_gdot = s_gold + MAX_SLIP * CONST_THREADS;
   double *s_g = s_gdot + MAX_SLIP * CONST_THREADS;
   double *s_epo = s_g + MAX_SLIP * CONST_THREADS;
@@ -290,11 +344,21 @@ __global__ void __launch_bounds__(CONST_THREADS, 3) constitutive_kernel(ConstArg
 #define TS(arr, k) arr[(k) * CONST_THREADS]
   __shared__ int blk_max;
   __shared__ int blk_fail;
-  {
+  const int per = const_items(V);
+  const int n_items = list_items(list, per);
+  int staged = -1;  // slot whose phase table is in shared memory
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+  const int kslot = item / per;
+  const int local = item - kslot * per;
+  const int slot = list.ids[kslot];
+  const ConstArgs<T> a = const_args<T>(tab[slot], V);
+  __syncthreads();
+  if (slot != staged) {
     const int nw = a.n_params * (int)(sizeof(PhaseParams) / sizeof(int));
     const int *src = reinterpret_cast<const int *>(a.params);
     int *dst = reinterpret_cast<int *>(sp);
     for (int i = tid; i < nw; i += CONST_THREADS) dst[i] = src[i];
+    staged = slot;
   }
   if (tid == 0) {
     blk_max = 0;
@@ -303,9 +367,8 @@ __global__ void __launch_bounds__(CONST_THREADS, 3) constitutive_kernel(ConstArg
   __syncthreads();
   int my_iters = 0;
   bool my_fail = false;
-  const long long V = a.V;
-  for (long long v = (long long)blockIdx.x * CONST_THREADS + tid; v < V;
-       v += (long long)gridDim.x * CONST_THREADS) {
+  const long long v1 = min(V, (long long)(local + 1) * CONST_POINTS);
+  for (long long v = (long long)local * CONST_POINTS + tid; v < v1; v += CONST_THREADS) {
     const int ph = a.phase ? a.phase[v] : 0;
     const PhaseParams &P = sp[ph];
     double eps[6];
@@ -355,6 +418,11 @@ __global__ void __launch_bounds__(CONST_THREADS, 3) constitutive_kernel(ConstArg
 #pragma unroll
           for (int j = i; j < 6; ++j) a.kvox[sym_idx(i, j) * V + v] = (T)P.C[i * 6 + j];
         a.g_out[v] = a.g_in[v];
+        // the trial plastic state equals the committed one, so that a commit may swap
+        // the trial and committed buffers
+#pragma unroll
+        for (int c = 0; c < 6; ++c) a.ep_trial[c * V + v] = epo[c];
+        a.Gam_trial[v] = eq_old;
         my_iters = max(my_iters, 1);
         continue;
       }
@@ -551,7 +619,6 @@ __global__ void __launch_bounds__(CONST_THREADS, 3) constitutive_kernel(ConstArg
     for (int c = 0; c < 6; ++c) a.ep_trial[c * V + v] = ep[c];
     a.Gam_trial[v] = Gold + dgam;
   }
-#undef TS
   if (my_iters) atomicMax(&blk_max, my_iters);
   if (my_fail) blk_fail = 1;
   __syncthreads();
@@ -559,4 +626,6 @@ __global__ void __launch_bounds__(CONST_THREADS, 3) constitutive_kernel(ConstArg
     atomicMax(a.max_iters, blk_max);
     if (blk_fail) atomicOr(a.failed, 1);
   }
+  }
+#undef TS
 }

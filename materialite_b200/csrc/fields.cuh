@@ -5,6 +5,8 @@
 
 #include "common.cuh"
 #include "constitutive.cuh"
+#include "krylov.cuh"
+#include "slots.cuh"
 
 // Tangent lookup: table mode (per (orientation, phase) pair) or voxel mode (21 planes).
 template <typename T> struct TangentRef {
@@ -37,55 +39,84 @@ template <typename T> struct TangentRef {
   }
 };
 
-struct StepVec {
-  double corr[6];  // tangent.mean().inv @ stress_increment, or zero
-  double dEbar[6]; // strain increment alone (first-step stress guess)
-  double dS[6];    // stress increment
-};
+// The slot's tangent: the committed one (start of a load increment: the tangent of the
+// last converged state, or the initial one) or the latest constitutive output.
+template <typename T>
+__device__ __forceinline__ TangentRef<T> tangent_of(const SlotDev<T> &S, bool committed,
+                                                    long long V) {
+  TangentRef<T> K;
+  K.ktab = S.ktab;
+  K.gid = S.gid;
+  K.kvox = S.voxel_mode ? (committed ? S.kvox_old : S.kvox) : nullptr;
+  K.V = V;
+  return K;
+}
 
 // strain = old_strain + dE + old_fluct ; guess = first ? dS + K dEbar : old_stress + dS
-// (small_strain_fft.py:113-123)
+// (small_strain_fft.py:113-123).  The guess goes to the slot's latest-stress buffer, which
+// the next constitutive call reads.  The fluctuation is first scaled by the slot's
+// fluct_scale (new dt / old dt after an increment, 1/2 after a cutback,
+// small_strain_fft.py:236-244) or cleared (reset_fluct: the load reversed).
 template <typename T>
 __global__ void __launch_bounds__(SSFFT_THREADS)
-    strain_guess_kernel(long long V, StepVec sv, int first_step, int reset_fluct,
-                        const T *__restrict__ eps_old, T *__restrict__ dfl,
-                        const T *__restrict__ sig_old, T *__restrict__ eps,
-                        T *__restrict__ guess, TangentRef<T> K) {
-  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < V;
-       v += (long long)gridDim.x * blockDim.x) {
+    strain_guess_kernel(const SlotDev<T> *__restrict__ tab, SlotList list, long long V) {
+  const int per = vec_items(V);
+  const int n_items = list_items(list, per);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int k = item / per;
+    const int local = item - k * per;
+    const SlotDev<T> &S = tab[list.ids[k]];
+    const long long v0 = (long long)local * VEC_CHUNK;
+    const long long v1 = min(V, v0 + VEC_CHUNK);
+    const StepVec sv = S.sv;
+    const bool first = S.first_step != 0, reset = S.reset_fluct != 0;
+    const double fs = S.fluct_scale;
+    const TangentRef<T> K = tangent_of<T>(S, true, V);
+    for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
 #pragma unroll
-    for (int c = 0; c < 6; ++c) {
-      T f = dfl[c * V + v];
-      if (reset_fluct) {
-        f = 0;
-        dfl[c * V + v] = 0;
+      for (int c = 0; c < 6; ++c) {
+        T f = S.dfl[c * V + v];
+        if (reset) f = 0;
+        else if (fs != 1.0) f = (T)((double)f * fs);
+        if (reset || fs != 1.0) S.dfl[c * V + v] = f;
+        // same association as the reference: (old + dEbar + fluct) + correction
+        double e = (double)S.eps_old[c * V + v] + sv.dEbar[c];
+        S.eps[c * V + v] = (T)((e + (double)f) + sv.corr[c]);
       }
-      // same association as the reference: (old + dEbar + fluct) + correction
-      double e = (double)eps_old[c * V + v] + sv.dEbar[c];
-      eps[c * V + v] = (T)((e + (double)f) + sv.corr[c]);
-    }
-    if (first_step) {
-      double y[6];
-      K.apply(v, sv.dEbar, y);
+      if (first) {
+        double y[6];
+        K.apply(v, sv.dEbar, y);
 #pragma unroll
-      for (int c = 0; c < 6; ++c) guess[c * V + v] = (T)(sv.dS[c] + y[c]);
-    } else {
+        for (int c = 0; c < 6; ++c) S.sig[c * V + v] = (T)(sv.dS[c] + y[c]);
+      } else {
 #pragma unroll
-      for (int c = 0; c < 6; ++c) guess[c * V + v] = (T)((double)sig_old[c * V + v] + sv.dS[c]);
+        for (int c = 0; c < 6; ++c)
+          S.sig[c * V + v] = (T)((double)S.sig_old[c * V + v] + sv.dS[c]);
+      }
     }
   }
 }
 
-// strain += dx ; old_fluct += dx  (small_strain_fft.py:154-155)
+// strain += dx ; old_fluct += dx  (small_strain_fft.py:154-155), dx the slot's Krylov
+// iterate.  (In the mixed mode the double re-projection of dx does this in its epilogue.)
 template <typename T>
 __global__ void __launch_bounds__(SSFFT_THREADS)
-    update_strain_kernel(long long n, const T *__restrict__ dx, T *__restrict__ eps,
-                         T *__restrict__ dfl) {
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const T d = dx[i];
-    eps[i] += d;
-    dfl[i] += d;
+    update_strain_kernel(const SlotDev<T> *__restrict__ tab, SlotList list, long long V) {
+  const long long n = 6 * V;
+  const int per = vec_items(n);
+  const int n_items = list_items(list, per);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int k = item / per;
+    const int local = item - k * per;
+    const SlotDev<T> &S = tab[list.ids[k]];
+    const T *dx = S.kr[5];
+    const long long i0 = (long long)local * VEC_CHUNK;
+    const long long i1 = min(n, i0 + VEC_CHUNK);
+    for (long long i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+      const T d = dx[i];
+      S.eps[i] += d;
+      S.dfl[i] += d;
+    }
   }
 }
 
@@ -105,9 +136,10 @@ __device__ __forceinline__ double dev_norm6(const double *s) {
 
 // Convergence quantities of small_strain_fft.py:172-189 in one pass:
 //   out[0..5]  sum of stress      out[6..11] sum of strain
-//   out[12]    max |dev(stress - old_stress)|   out[13] max |K : dx|  (if dx given)
+//   out[12]    max |dev(stress - old_stress)|   out[13] max |K : dx|  (if norms_dx)
 #define NORM_VALS 14
 #define NORM_SUMS 12  // values 0..11 are sums, 12..13 maxima
+#define NORM_CHUNK (4 * SSFFT_THREADS)  // points per item
 
 // Combine one of the norm values (sum or max) in a fixed order.
 __device__ __forceinline__ double norm_combine(int k, double a, double b) {
@@ -121,89 +153,134 @@ __device__ __forceinline__ double norm_warp_reduce(int k, double v) {
   return v;
 }
 
+__host__ __device__ inline int norm_items(long long V) { return (int)((V + NORM_CHUNK - 1) / NORM_CHUNK); }
+
 template <typename T>
 __global__ void __launch_bounds__(SSFFT_THREADS)
-    newton_norms_kernel(long long V, const T *__restrict__ sig, const T *__restrict__ sig_old,
-                        const T *__restrict__ eps, const T *__restrict__ dx, TangentRef<T> K,
-                        double *partials, unsigned int *ticket, double *out) {
+    newton_norms_kernel(const SlotDev<T> *__restrict__ tab, SlotList list, long long V) {
   __shared__ double wred[NORM_VALS][SSFFT_THREADS / 32];
-  double acc[NORM_VALS];
-#pragma unroll
-  for (int k = 0; k < NORM_VALS; ++k) acc[k] = 0.0;
-  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < V;
-       v += (long long)gridDim.x * blockDim.x) {
-    double s[6], d[6];
-#pragma unroll
-    for (int c = 0; c < 6; ++c) {
-      s[c] = (double)sig[c * V + v];
-      acc[c] += s[c];
-      acc[6 + c] += (double)eps[c * V + v];
-      d[c] = s[c] - (double)sig_old[c * V + v];
-    }
-    acc[12] = fmax(acc[12], dev_norm6(d));
-    if (dx) {
-      double x[6], y[6];
-#pragma unroll
-      for (int c = 0; c < 6; ++c) x[c] = (double)dx[c * V + v];
-      K.apply(v, x, y);
-      double n2 = 0.0;
-#pragma unroll
-      for (int c = 0; c < 6; ++c) n2 += y[c] * y[c];
-      acc[13] = fmax(acc[13], sqrt(n2));
-    }
-  }
-  // all fourteen values through one warp pass and one barrier
+  const int per = norm_items(V);
+  const int n_items = list_items(list, per);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int kslot = item / per;
+    const int local = item - kslot * per;
+    const SlotDev<T> &S = tab[list.ids[kslot]];
+    const T *dx = S.norms_dx ? S.kr[5] : nullptr;
+    const TangentRef<T> K = tangent_of<T>(S, false, V);
+    double acc[NORM_VALS];
 #pragma unroll
-  for (int k = 0; k < NORM_VALS; ++k) {
-    const double r = norm_warp_reduce(k, acc[k]);
-    if (lane == 0) wred[k][warp] = r;
+    for (int k = 0; k < NORM_VALS; ++k) acc[k] = 0.0;
+    const long long v0 = (long long)local * NORM_CHUNK;
+    const long long v1 = min(V, v0 + NORM_CHUNK);
+    for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
+      double s[6], d[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        s[c] = (double)S.sig[c * V + v];
+        acc[c] += s[c];
+        acc[6 + c] += (double)S.eps[c * V + v];
+        d[c] = s[c] - (double)S.sig_old[c * V + v];
+      }
+      acc[12] = fmax(acc[12], dev_norm6(d));
+      if (dx) {
+        double x[6], y[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) x[c] = (double)dx[c * V + v];
+        K.apply(v, x, y);
+        double n2 = 0.0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) n2 += y[c] * y[c];
+        acc[13] = fmax(acc[13], sqrt(n2));
+      }
+    }
+    // all fourteen values through one warp pass and one barrier
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NORM_VALS; ++k) {
+      const double r = norm_warp_reduce(k, acc[k]);
+      if (lane == 0) wred[k][warp] = r;
+    }
+    __syncthreads();
+    if (threadIdx.x < NORM_VALS) {
+      const int k = threadIdx.x;
+      double r = wred[k][0];
+      for (int w = 1; w < nw; ++w) r = norm_combine(k, r, wred[k][w]);
+      S.partials[(size_t)local * NORM_VALS + k] = r;
+    }
+    if (last_item_arrives(S.tickets + TK_NORMS, (unsigned)per)) {
+      // one warp per value: lanes stride over the item partials, then a fixed tree
+      for (int k = warp; k < NORM_VALS; k += nw) {
+        double r = 0.0;
+        for (int b = lane; b < per; b += 32)
+          r = norm_combine(k, r, S.partials[(size_t)b * NORM_VALS + k]);
+        r = norm_warp_reduce(k, r);
+        if (lane == 0) S.results[k] = r;
+      }
+      if (threadIdx.x == 0) S.tickets[TK_NORMS] = 0;
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  if (threadIdx.x < NORM_VALS) {
-    const int k = threadIdx.x;
-    double r = wred[k][0];
-    for (int w = 1; w < nw; ++w) r = norm_combine(k, r, wred[k][w]);
-    partials[(size_t)blockIdx.x * NORM_VALS + k] = r;
-  }
-  if (!last_block_arrives(ticket)) return;
-  // one warp per value: lanes stride over the block partials, then a fixed tree
-  for (int k = warp; k < NORM_VALS; k += nw) {
-    double r = 0.0;
-    for (int b = lane; b < (int)gridDim.x; b += 32)
-      r = norm_combine(k, r, partials[(size_t)b * NORM_VALS + k]);
-    r = norm_warp_reduce(k, r);
-    if (lane == 0) out[k] = r;
-  }
-  if (threadIdx.x == 0) *ticket = 0;
 }
 
-// Sum of the tangent over all points (21 packed entries) for tangent.mean().inv
-// (small_strain_fft.py:119-120).
+// Sum of the committed tangent over all points (21 packed entries) for
+// tangent.mean().inv (small_strain_fft.py:119-120), into results[16..36].
 template <typename T>
 __global__ void __launch_bounds__(SSFFT_THREADS)
-    tangent_sum_kernel(long long V, TangentRef<T> K, double *partials, unsigned int *ticket,
-                       double *out) {
+    tangent_sum_kernel(const SlotDev<T> *__restrict__ tab, SlotList list, long long V) {
   __shared__ double red[32];
-  double acc[21];
+  const int per = vec_items(V);
+  const int n_items = list_items(list, per);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int kslot = item / per;
+    const int local = item - kslot * per;
+    const SlotDev<T> &S = tab[list.ids[kslot]];
+    const TangentRef<T> K = tangent_of<T>(S, true, V);
+    double acc[21];
 #pragma unroll
-  for (int k = 0; k < 21; ++k) acc[k] = 0.0;
-  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < V;
-       v += (long long)gridDim.x * blockDim.x) {
+    for (int k = 0; k < 21; ++k) acc[k] = 0.0;
+    const long long v0 = (long long)local * VEC_CHUNK;
+    const long long v1 = min(V, v0 + VEC_CHUNK);
+    for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
 #pragma unroll
-    for (int k = 0; k < 21; ++k) acc[k] += K.entry(v, k);
-  }
+      for (int k = 0; k < 21; ++k) acc[k] += K.entry(v, k);
+    }
 #pragma unroll
-  for (int k = 0; k < 21; ++k) {
-    const double r = block_sum(acc[k], red);
-    if (threadIdx.x == 0) partials[(size_t)blockIdx.x * 21 + k] = r;
+    for (int k = 0; k < 21; ++k) {
+      const double r = block_sum(acc[k], red);
+      if (threadIdx.x == 0) S.partials[(size_t)local * 21 + k] = r;
+    }
+    if (last_item_arrives(S.tickets + TK_TSUM, (unsigned)per)) {
+      for (int k = 0; k < 21; ++k) {
+        const double r = ordered_sum(S.partials + k, per, 21, red);
+        if (threadIdx.x == 0) S.results[16 + k] = r;
+      }
+      if (threadIdx.x == 0) S.tickets[TK_TSUM] = 0;
+    }
+    __syncthreads();
   }
-  if (!last_block_arrives(ticket)) return;
-  for (int k = 0; k < 21; ++k) {
-    const double r = ordered_sum(partials + k, gridDim.x, 21, red);
-    if (threadIdx.x == 0) out[k] = r;
+}
+
+// Commit of the slip resistances (elastic_viscoplastic.py:264-266): g_old = g_in, the last
+// converged trial.  The other committed fields change roles by pointer swaps; g_in must
+// keep its values, since the next constitutive call starts its inner Newton from them.
+template <typename T>
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    commit_slip_kernel(const SlotDev<T> *__restrict__ tab, SlotList list, long long V,
+                       int nslip_max) {
+  const long long n = (long long)nslip_max * V;
+  const int per = vec_items(n);
+  const int n_items = list_items(list, per);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int k = item / per;
+    const int local = item - k * per;
+    const SlotDev<T> &S = tab[list.ids[k]];
+    if (!S.any_evp) continue;
+    const long long ns = (long long)S.nslip * V;
+    const long long i0 = (long long)local * VEC_CHUNK;
+    const long long i1 = min(ns, i0 + VEC_CHUNK);
+    for (long long i = i0 + threadIdx.x; i < i1; i += blockDim.x) S.g_old[i] = S.g_in[i];
   }
-  if (threadIdx.x == 0) *ticket = 0;
 }
 
 // Planar T (width planes of V) -> point-major float64 (V x width).

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 #include <string>
 
@@ -36,9 +37,16 @@
 #define NOALLOC_MAX_AXIS 1024
 #define NOALLOC_MAX_DEVICES 64
 #define NOALLOC_TABLE_OFFSET (6 * NOALLOC_MAX_SPEC_POINTS)
-#define NOALLOC_ELEMS (NOALLOC_TABLE_OFFSET + 3 * NOALLOC_MAX_AXIS + 2 * NOALLOC_MAX_AXIS)
+#define NOALLOC_DESC_OFFSET (NOALLOC_TABLE_OFFSET + 3 * NOALLOC_MAX_AXIS + 2 * NOALLOC_MAX_AXIS)
+#define NOALLOC_DESC_ELEMS 64  // room for the one-slot descriptor
+#define NOALLOC_LIST_OFFSET (NOALLOC_DESC_OFFSET + NOALLOC_DESC_ELEMS)
+#define NOALLOC_ELEMS (NOALLOC_LIST_OFFSET + 1)
 
-// spectrum (6 components), then 3 twiddle tables (double2), then 3 tan tables (double)
+static_assert(sizeof(SlotDev<double>) <= NOALLOC_DESC_ELEMS * sizeof(double2),
+              "slot descriptor does not fit its scratch space");
+
+// spectrum (6 components), then 3 twiddle tables (double2), then 3 tan tables (double),
+// then the slot descriptor the transform kernels read and the slot list {0, 1}
 static __device__ __align__(256) double2 g_noalloc_scratch[NOALLOC_ELEMS];
 
 // Failure messages go to ssfft_last_error() (defined in ssfft.cu).
@@ -86,9 +94,12 @@ static int noalloc_setup(int dev, double2 **out) {
     cudaError_t a[5] = {
         cudaFuncSetAttribute(zfwd_kernel<double, double, PRO_INPUT>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, m),
-        cudaFuncSetAttribute(ypass_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, m),
-        cudaFuncSetAttribute(xpass_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, m),
-        cudaFuncSetAttribute(ypass_kernel<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, m),
+        cudaFuncSetAttribute(ypass_kernel<double, double, false, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, m),
+        cudaFuncSetAttribute(xpass_kernel<double, double, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, m),
+        cudaFuncSetAttribute(ypass_kernel<double, double, true, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, m),
         cudaFuncSetAttribute(zinv_kernel<double, double, EPI_STORE>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, m)};
     for (cudaError_t x : a)
@@ -137,7 +148,7 @@ extern "C" int ssfft_apply_projection_noalloc(const int32_t n[3], const double s
   g.nz = nz;
   g.hz = hz;
   g.V = (long long)nx * ny * nz;
-  g.S = S;
+  g.S = (long long)nx * ny * ((nz % 2 == 0) ? nz / 2 : hz);  // stored columns (no Nyquist)
   g.twx = tw;
   g.twy = tw + NOALLOC_MAX_AXIS;
   g.twz = tw + 2 * NOALLOC_MAX_AXIS;
@@ -145,7 +156,6 @@ extern "C" int ssfft_apply_projection_noalloc(const int32_t n[3], const double s
   g.tany = tn + NOALLOC_MAX_AXIS;
   g.tanz = tn + 2 * NOALLOC_MAX_AXIS;
   g.scale = 1.0 / (double)g.V;
-  for (int c = 0; c < 6; ++c) g.mask[c] = stress_mask[c];
   // tiles of the handle-based path's double-precision transforms, except that the x pass
   // always takes 8 kz columns per block (the handle path takes 4 on axes of up to 64)
   g.lz = nz >= 3 * 2048 ? 1 : std::max(1, std::min(32, 2048 / (3 * nz)));
@@ -160,19 +170,31 @@ extern "C" int ssfft_apply_projection_noalloc(const int32_t n[3], const double s
   const size_t sx = smem_x_bytes<double>(g.kx, nx);
   if (sz > 200 * 1024 || sy > 200 * 1024 || sx > 200 * 1024)
     return noalloc_fail(SSFFT_E_UNSUPPORTED, "grid too large for the shared-memory FFT passes");
-  ProArgs<double> pa{};
-  pa.in = in_dev;
-  EpiArgs<double> ea{};
-  ea.out = out_dev;
-  const int nzb = (int)(((long long)nx * ny + g.lz - 1) / g.lz);
+  // the one-slot descriptor: the transforms read the spectrum and the stress mask from it
+  SlotDev<double> desc;
+  memset((void *)&desc, 0, sizeof(desc));
+  desc.spec = spec;
+  for (int c = 0; c < 6; ++c) desc.mask[c] = stress_mask[c];
+  SlotDev<double> *dtab = reinterpret_cast<SlotDev<double> *>(base + NOALLOC_DESC_OFFSET);
+  int *dlist = reinterpret_cast<int *>(base + NOALLOC_LIST_OFFSET);
+  const int list[2] = {0, 1};
+  e = cudaMemcpyAsync(dtab, &desc, sizeof(desc), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dlist, list, sizeof(list), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess)
+    return noalloc_fail(SSFFT_E_CUDA, std::string("projection set-up: ") + cudaGetErrorString(e));
+  SlotList L;
+  L.ids = dlist;
+  L.count = dlist + 1;
+  ExtIO<double> io;
+  io.in = in_dev;
+  io.out = out_dev;
+  // one block per item of the single slot
   noalloc_tables_kernel<<<1, 256, 0, s>>>(nx, ny, nz, tw, tn);
-  zfwd_kernel<double, double, PRO_INPUT><<<nzb, SSFFT_THREADS, sz, s>>>(g, pa, spec);
-  ypass_kernel<double, false><<<dim3((hz + g.ky - 1) / g.ky, nx, 6), SSFFT_THREADS, sy, s>>>(
-      g, spec, nullptr);
-  xpass_kernel<double><<<dim3((hz + g.kx - 1) / g.kx, ny), SSFFT_THREADS, sx, s>>>(g, spec, nullptr);
-  ypass_kernel<double, true><<<dim3((hz + g.ky - 1) / g.ky, nx, 6), SSFFT_THREADS, sy, s>>>(
-      g, spec, nullptr);
-  zinv_kernel<double, double, EPI_STORE><<<nzb, SSFFT_THREADS, sz, s>>>(g, ea, spec);
+  zfwd_kernel<double, double, PRO_INPUT><<<items_z(g), SSFFT_THREADS, sz, s>>>(g, dtab, L, io);
+  ypass_kernel<double, double, false, false><<<items_y(g), SSFFT_THREADS, sy, s>>>(g, dtab, L);
+  xpass_kernel<double, double, false><<<items_x(g), SSFFT_THREADS, sx, s>>>(g, dtab, L);
+  ypass_kernel<double, double, true, false><<<items_y(g), SSFFT_THREADS, sy, s>>>(g, dtab, L);
+  zinv_kernel<double, double, EPI_STORE><<<items_z(g), SSFFT_THREADS, sz, s>>>(g, dtab, L, io);
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess)

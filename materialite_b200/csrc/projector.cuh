@@ -1,12 +1,15 @@
 // The compatibility projection  out = ifftn( Gamma-hat(q) : fftn(tau) ).real  of
-// materialite's SmallStrainFFT (small_strain_fft.py:301-382), as five passes over a
-// half spectrum held in HBM:
+// materialite's SmallStrainFFT (small_strain_fft.py:301-382), over a half spectrum held in
+// HBM, for every slot of a SlotList at once.
 //
-//   zfwd : per (x,y) line, build tau (prologue), real-to-complex FFT along z
+// Five passes (any grid):
+//   zfwd : per tile of (x,y) lines, build tau (prologue), real-to-complex FFT along z
 //   yfwd : complex FFT along y
 //   xpass: complex FFT along x, Gamma-hat apply on all six components, inverse along x
 //   yinv : inverse complex FFT along y
 //   zinv : complex-to-real inverse along z, then the epilogue
+// Three passes (grids whose yz plane fits in shared memory): zyfwd does z and y of one x
+// plane, yzinv their inverse, and the spectrum crosses HBM four times instead of eight.
 //
 // The six real components are paired into three complex lines for the z passes
 // ((0,1), (2,3), (4,5)), so the z transforms run at half length-cost.  Gamma-hat is
@@ -15,58 +18,86 @@
 // reduces exactly to  Gamma-hat : T = t (x) u + u (x) t - (t . u) t (x) t,  u = T t.
 // Nyquist planes of even sizes are zero (small_strain_fft.py:354-359) and
 // Gamma-hat(0) = diag(stress_mask) (:363-367).
+//
+// Every kernel runs a persistent grid over items (slot, tile); see slots.cuh.
 #pragma once
 
 #include "common.cuh"
 #include "fft.cuh"
+#include "slots.cuh"
 
-// Spectrum layout: spec[c * S + (x * ny + y) * hz + kz], c = Mandel component,
-// hz = nz/2 + 1, S = nx * ny * hz.  Real fields: f[c * V + (x * ny + y) * nz + z].
+// Spectrum layout: spec[c * S + (x * ny + y) * hs + kz], c = Mandel component,
+// S = nx * ny * hs.  Real fields: f[c * V + (x * ny + y) * nz + z].  The half spectrum
+// has hz = nz/2 + 1 columns; on even grids the last one, kz = nz/2, is a Nyquist plane that
+// Gamma-hat zeroes (small_strain_fft.py:354-359), so it is neither stored nor transformed
+// along x and y: hs = nz/2 columns are stored (hs = hz on odd grids), and the inverse
+// z passes read the Nyquist column as zero.
 template <typename T> struct Grid {
-  int nx, ny, nz, hz;
+  int nx, ny, nz, hz, hs;
   long long V, S;
   AxisPlan px, py, pz;
   const cplx<T> *twx, *twy, *twz;  // e^{-2 pi i k / n}, k < n
   const T *tanx, *tany, *tanz;     // tan(pi f_k) with f = fftfreq (nx, ny, hz entries)
   T scale;                         // 1 / V
-  T mask[6];                       // stress mask (0/1)
-  int lz;                          // (x,y) lines per z-pass block
-  int ky;                          // kz columns per y-pass block
-  int kx;                          // kz columns per x-pass block
+  int lz;                          // (x,y) lines per z-pass tile
+  int ky;                          // kz columns per y-pass tile
+  int kx;                          // kz columns per x-pass tile
+  int nzb, nky, nkx;               // tiles along the lines, y columns and x columns
   // Divisors of the index arithmetic, prepared on the host (grid_divisors): [0] for a full
   // tile, [1] for the last, partial one along that axis.
-  FastDiv fd_nz, fd_hz, fd_ny, fd_2hz, fd_plane;  // plane kernels: nz, hz, ny, 2 hz, ny hz
-  FastDiv fd_z3[2], fd_znh[2], fd_znz[2];        // z passes: 3 nl, nl hz, nl nz
-  FastDiv fd_ky[2];                              // y passes: nk
-  FastDiv fd_kx[2], fd_x6k[2], fd_xslab[2];      // x pass: nk, 6 nk, nx nk
+  FastDiv fd_nz, fd_hs, fd_ny, fd_nx, fd_2hs, fd_plane;  // plane kernels
+  FastDiv fd_z3[2], fd_znh[2], fd_znz[2];               // z passes: 3 nl, nl hs, nl nz
+  FastDiv fd_ky[2];                                     // y passes: nk
+  FastDiv fd_kx[2], fd_x6k[2], fd_xslab[2];             // x pass: nk, 6 nk, nx nk
+  // items per slot and their decomposition
+  FastDiv fd_it_plane, fd_it_x, fd_nkx, fd_it_z, fd_it_y, fd_nky, fd_nkynx, fd_3;
 };
 
-// Fill the divisor table of a grid whose sizes and tiles (lz, ky, kx) are set.
+// Fill the stored-column count, tile counts and divisor table of a grid whose sizes and
+// tiles (lz, ky, kx) are set.
 template <typename T> inline void grid_divisors(Grid<T> &g) {
   const long long lines = (long long)g.nx * g.ny;
-  const int nzb = (int)((lines + g.lz - 1) / g.lz);
-  const int lzt = (int)(lines - (long long)(nzb - 1) * g.lz);
-  const int kyt = g.hz - ((g.hz + g.ky - 1) / g.ky - 1) * g.ky;
-  const int kxt = g.hz - ((g.hz + g.kx - 1) / g.kx - 1) * g.kx;
+  g.hs = (g.nz % 2 == 0) ? g.nz / 2 : g.hz;
+  g.nzb = (int)((lines + g.lz - 1) / g.lz);
+  g.nky = (g.hs + g.ky - 1) / g.ky;
+  g.nkx = (g.hs + g.kx - 1) / g.kx;
+  const int lzt = (int)(lines - (long long)(g.nzb - 1) * g.lz);
+  const int kyt = g.hs - (g.nky - 1) * g.ky;
+  const int kxt = g.hs - (g.nkx - 1) * g.kx;
   auto fd = [](long long d) { return make_fastdiv((uint32_t)d); };
   g.fd_nz = fd(g.nz);
-  g.fd_hz = fd(g.hz);
+  g.fd_hs = fd(g.hs);
   g.fd_ny = fd(g.ny);
-  g.fd_2hz = fd(2 * g.hz);
-  g.fd_plane = fd((long long)g.ny * g.hz);
+  g.fd_nx = fd(g.nx);
+  g.fd_2hs = fd(2 * g.hs);
+  g.fd_plane = fd((long long)g.ny * g.hs);
   const int nl[2] = {g.lz, lzt}, ky[2] = {g.ky, kyt}, kx[2] = {g.kx, kxt};
   for (int t = 0; t < 2; ++t) {
     g.fd_z3[t] = fd(3LL * nl[t]);
-    g.fd_znh[t] = fd((long long)nl[t] * g.hz);
+    g.fd_znh[t] = fd((long long)nl[t] * g.hs);
     g.fd_znz[t] = fd((long long)nl[t] * g.nz);
     g.fd_ky[t] = fd(ky[t]);
     g.fd_kx[t] = fd(kx[t]);
     g.fd_x6k[t] = fd(6LL * kx[t]);
     g.fd_xslab[t] = fd((long long)g.nx * kx[t]);
   }
+  g.fd_it_plane = fd(3LL * g.nx);
+  g.fd_it_x = fd((long long)g.nkx * g.ny);
+  g.fd_nkx = fd(g.nkx);
+  g.fd_it_z = fd(g.nzb);
+  g.fd_it_y = fd(6LL * g.nky * g.nx);
+  g.fd_nky = fd(g.nky);
+  g.fd_nkynx = fd((long long)g.nky * g.nx);
+  g.fd_3 = fd(3);
 }
 
 __device__ __forceinline__ int udiv(int n, const FastDiv &f) { return (int)fdiv((uint32_t)n, f); }
+
+// Items of one slot in each pass.
+template <typename T> __host__ __device__ inline int items_plane(const Grid<T> &g) { return 3 * g.nx; }
+template <typename T> __host__ __device__ inline int items_x(const Grid<T> &g) { return g.nkx * g.ny; }
+template <typename T> __host__ __device__ inline int items_z(const Grid<T> &g) { return g.nzb; }
+template <typename T> __host__ __device__ inline int items_y(const Grid<T> &g) { return 6 * g.nky * g.nx; }
 
 // Shared-memory footprint of the passes (elements of cplx<T>).  The z passes hold three
 // paired lines per (x,y) line, padded (sidx<true>); the x pass pads each component slab
@@ -95,27 +126,29 @@ struct MinresState {
   int istop, done;
 };
 
-// ---- prologue modes of zfwd ----------------------------------------------------------
-enum { PRO_INPUT = 0, PRO_RESIDUAL = 1, PRO_TANGENT_TABLE = 2, PRO_TANGENT_VOXEL = 3 };
-
-template <typename T> struct ProArgs {
-  const T *in;           // PRO_INPUT: tau planes; PRO_RESIDUAL: stress; TANGENT: Lanczos u_j
-  const int32_t *gid;    // TANGENT_TABLE: tangent index per point
-  const T *ktab;         // TANGENT_TABLE: [n_gid][21]
-  const T *kvox;         // TANGENT_VOXEL: 21 planes of V
-  MinresState *st;       // TANGENT_*: scalars, early exit when done
-  double sbar[6];        // PRO_RESIDUAL: applied mean stress
-  // TANGENT_*: the MINRES vector update of the previous iteration, applied here
-  const T *y;            // y' of the previous iteration
-  T *unew;               // receives u_{j+1} = y' - (alfa/beta) u_j
-  const T *w1, *w2;      // the two previous search directions
-  T *wout;               // receives the new direction
-  T *x;                  // the iterate, updated in place
-  double *partials;      // per-block |x|^2
-  unsigned int *ticket;  // last-block counter of the |x|^2 reduction
+// Caller-owned input and output of the plain projection (PRO_INPUT / EPI_STORE).
+template <typename TF> struct ExtIO {
+  const TF *in;
+  TF *out;
 };
 
-// Stopping tests of scipy's minres after the solution update (last block of the forward
+// ---- prologue modes of the forward passes ---------------------------------------------
+//   PRO_INPUT          tau = caller's planes
+//   PRO_RESIDUAL       tau = Sbar - sigma                    (small_strain_fft.py:140,168)
+//   PRO_TANGENT_*      tau = K v of the Krylov iteration     (:370-374), table or voxel K
+//   PRO_REPROJECT      tau = x (the Newton correction)
+enum { PRO_INPUT = 0, PRO_RESIDUAL = 1, PRO_TANGENT_TABLE = 2, PRO_TANGENT_VOXEL = 3,
+       PRO_REPROJECT = 4 };
+#define PRO_IS_KRYLOV(P) ((P) == PRO_TANGENT_TABLE || (P) == PRO_TANGENT_VOXEL)
+
+// ---- epilogue modes of the inverse passes -----------------------------------------------
+//   EPI_STORE          caller's planes = result
+//   EPI_RESIDUAL       b = result, max|b|                    (:141-144)
+//   EPI_MINRES         y' and the MINRES recurrence          (krylov.cuh)
+//   EPI_REPROJECT      x = result; strain += x; fluctuation += x   (:154-155)
+enum { EPI_STORE = 0, EPI_RESIDUAL = 1, EPI_MINRES = 2, EPI_REPROJECT = 3 };
+
+// Stopping tests of scipy's minres after the solution update (last item of the forward
 // pass that applied it, with x2 = |x|^2).
 static __device__ __noinline__ void minres_after_update(MinresState *st, double x2) {
   MinresState s = *st;
@@ -141,18 +174,57 @@ static __device__ __noinline__ void minres_after_update(MinresState *st, double 
   *st = s;
 }
 
-// Scalars of the update pending from the previous MINRES iteration, read once per thread
-// (all iterations after the first: itn >= 1).
-template <typename T> struct PendingUpdate {
+// MINRES scalar recurrence after the matvec (Paige & Saunders 1975; scipy's minres loop
+// body up to the plane rotation).  d0 = r2 . y', d1 = y' . y', d2 = r2 . r2 where
+// y' = A v - (beta/oldb) r1 and v = r2 / beta.  The orthogonalised y'' = y' - (alfa/beta) r2
+// is formed by the next forward pass; its norm follows from the three dot products:
+// |y''|^2 = d1 - 2 c d0 + c^2 d2 with c = alfa / beta.
+static __device__ __noinline__ void minres_after_matvec(MinresState *st, double d0, double d1,
+                                                        double d2) {
+  MinresState s = *st;
+  s.itn += 1;
+  s.alfa = s.s * d0;
+  s.coef = s.alfa / s.beta;
+  double beta2 = d1 - 2.0 * s.coef * d0 + s.coef * s.coef * d2;
+  if (beta2 < 0.0) beta2 = 0.0;
+  s.oldb = s.beta;
+  s.beta = sqrt(beta2);
+  s.tnorm2 += s.alfa * s.alfa + s.oldb * s.oldb + s.beta * s.beta;
+  if (s.itn == 1 && s.beta / s.beta1 <= 10.0 * s.eps) s.istop = -1;
+  s.oldeps = s.epsln;
+  s.delta = s.cs * s.dbar + s.sn * s.alfa;
+  const double gbar = s.sn * s.dbar - s.cs * s.alfa;
+  s.epsln = s.sn * s.beta;
+  s.dbar = -s.cs * s.beta;
+  s.root = hypot(gbar, s.dbar);
+  s.gamma = fmax(hypot(gbar, s.beta), s.eps);
+  s.cs = gbar / s.gamma;
+  s.sn = s.beta / s.gamma;
+  s.phi = s.cs * s.phibar;
+  s.phibar = s.sn * s.phibar;
+  s.denom = 1.0 / s.gamma;
+  s.gmax = fmax(s.gmax, s.gamma);
+  s.gmin = fmin(s.gmin, s.gamma);
+  s.s_prev = s.s;
+  s.s = (s.beta > 0.0) ? 1.0 / s.beta : 0.0;
+  s.c_r1 = (s.oldb > 0.0) ? s.beta / s.oldb : 0.0;
+  *st = s;
+}
+
+// Scalars of the update pending from the previous MINRES iteration (all iterations after
+// the first: itn >= 1), and the vector roles of this iteration.
+template <typename T, typename TF> struct KrylovIn {
   bool on;
   T s, coef, sp, oe, de, dn, ph;
+  KRoles<TF> r;
 };
 
 template <typename T, typename TF>
-__device__ __forceinline__ PendingUpdate<T> pending_update(const ProArgs<TF> &a) {
-  const MinresState *st = a.st;
-  PendingUpdate<T> u;
-  u.on = st->itn >= 1;
+__device__ __forceinline__ KrylovIn<T, TF> krylov_in(const SlotDev<TF> &S) {
+  const MinresState *st = S.st;
+  KrylovIn<T, TF> u;
+  const long long itn = st->itn;
+  u.on = itn >= 1;
   u.s = (T)st->s;
   u.coef = (T)st->coef;
   u.sp = (T)st->s_prev;
@@ -160,6 +232,7 @@ __device__ __forceinline__ PendingUpdate<T> pending_update(const ProArgs<TF> &a)
   u.de = (T)st->delta;
   u.dn = (T)st->denom;
   u.ph = (T)st->phi;
+  u.r = kroles<TF>(S, itn);
   return u;
 }
 
@@ -176,24 +249,20 @@ __device__ __forceinline__ void sym6_apply(const T *k, long long kstride, const 
   }
 }
 
+// Non-Krylov prologues at one point.
 template <typename T, typename TF, int PRO>
-__device__ __forceinline__ void prologue(const Grid<T> &g, const ProArgs<TF> &a, long long v,
-                                         T s, T *tau) {
+__device__ __forceinline__ void prologue(const SlotDev<TF> &S, const TF *ext_in, long long V,
+                                         long long v, T *tau) {
   if constexpr (PRO == PRO_INPUT) {
 #pragma unroll
-    for (int c = 0; c < 6; ++c) tau[c] = (T)a.in[c * g.V + v];
-  } else if constexpr (PRO == PRO_RESIDUAL) {
+    for (int c = 0; c < 6; ++c) tau[c] = (T)ext_in[c * V + v];
+  } else if constexpr (PRO == PRO_REPROJECT) {
+    const TF *x = S.kr[5];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) tau[c] = (T)a.sbar[c] - (T)a.in[c * g.V + v];
+    for (int c = 0; c < 6; ++c) tau[c] = (T)x[c * V + v];
   } else {
-    T x[6];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) x[c] = s * a.in[c * g.V + v];
-    if constexpr (PRO == PRO_TANGENT_TABLE) {
-      sym6_apply<T>(a.ktab + (long long)a.gid[v] * 21, 1, x, tau);
-    } else {
-      sym6_apply<T>(a.kvox + v, g.V, x, tau);
-    }
+    for (int c = 0; c < 6; ++c) tau[c] = (T)S.sbar[c] - (T)S.sig[c * V + v];
   }
 }
 
@@ -205,24 +274,24 @@ __device__ __forceinline__ void prologue(const Grid<T> &g, const ProArgs<TF> &a,
 // ALL, tau[0..5] is the whole tau; otherwise tau[0..1] are the owned pair's components,
 // and only the two tangent rows they need are loaded.
 template <typename T, typename TF, int PRO, bool ALL>
-__device__ __forceinline__ void tangent_prologue(const Grid<T> &g, const ProArgs<TF> &a,
-                                                 long long v, const PendingUpdate<T> &u,
-                                                 int pair, T *tau, double &xx) {
+__device__ __forceinline__ void tangent_prologue(const SlotDev<TF> &S, long long V, long long v,
+                                                 const KrylovIn<T, TF> &u, int pair, T *tau,
+                                                 double &xx) {
   constexpr int NO = ALL ? 6 : 2;  // owned components
   const int c0 = ALL ? 0 : 2 * pair;
-  const long long V = g.V;
   // every load is issued before the first store: the stores may alias the loaded arrays
   // as far as the compiler knows, and loads held back behind them would serialise
   T r[6], yv[6], a1[NO], a2[NO], xo[NO], k[ALL ? 21 : 12];
+  const TF *in = u.r.P;
 #pragma unroll
-  for (int c = 0; c < 6; ++c) r[c] = (T)a.in[c * V + v];
+  for (int c = 0; c < 6; ++c) r[c] = (T)in[c * V + v];
   const TF *kp;
   long long ks;
   if constexpr (PRO == PRO_TANGENT_TABLE) {
-    kp = a.ktab + (long long)a.gid[v] * 21;
+    kp = S.ktab + (long long)S.gid[v] * 21;
     ks = 1;
   } else {
-    kp = a.kvox + v;
+    kp = S.kvox + v;
     ks = V;
   }
   if constexpr (ALL) {
@@ -236,13 +305,13 @@ __device__ __forceinline__ void tangent_prologue(const Grid<T> &g, const ProArgs
   }
   if (u.on) {
 #pragma unroll
-    for (int c = 0; c < 6; ++c) yv[c] = (T)a.y[c * V + v];
+    for (int c = 0; c < 6; ++c) yv[c] = (T)u.r.Y[c * V + v];
 #pragma unroll
     for (int q = 0; q < NO; ++q) {
       const long long i = (c0 + q) * V + v;
-      a1[q] = (T)a.w1[i];
-      a2[q] = (T)a.w2[i];
-      xo[q] = (T)a.x[i];
+      a1[q] = (T)u.r.W1[i];
+      a2[q] = (T)u.r.W2[i];
+      xo[q] = (T)u.r.X[i];
     }
   }
   T vv[6];
@@ -267,9 +336,9 @@ __device__ __forceinline__ void tangent_prologue(const Grid<T> &g, const ProArgs
       const long long i = (c0 + q) * V + v;
       const T w = (u.sp * ro - u.oe * a1[q] - u.de * a2[q]) * u.dn;
       const T xn = xo[q] + u.ph * w;
-      a.unew[i] = (TF)uo;
-      a.wout[i] = (TF)w;
-      a.x[i] = (TF)xn;
+      u.r.Q[i] = (TF)uo;
+      u.r.W[i] = (TF)w;
+      u.r.X[i] = (TF)xn;
       xx += (double)xn * (double)xn;
     }
   } else {
@@ -289,18 +358,18 @@ __device__ __forceinline__ void tangent_prologue(const Grid<T> &g, const ProArgs
   }
 }
 
-// End of a forward pass that applied a pending update: |x|^2 over all blocks, then the
-// stopping tests in the last block to arrive.
+// End of a forward item that applied a pending update: the slot's |x|^2 over its items,
+// then the stopping tests in the slot's last item to arrive.
 template <typename TF>
-__device__ __forceinline__ void finish_pending_update(const ProArgs<TF> &a, double xx, int blk,
-                                                      int nblk, double *red) {
+__device__ __forceinline__ void finish_pending_update(const SlotDev<TF> &S, double xx, int local,
+                                                      int per_slot, double *red) {
   const double part = block_sum(xx, red);
-  if (threadIdx.x == 0) a.partials[blk] = part;
-  if (!last_block_arrives(a.ticket)) return;
-  const double x2 = ordered_sum(a.partials, nblk, 1, red);
+  if (threadIdx.x == 0) S.partials[local] = part;
+  if (!last_item_arrives(S.tickets + TK_UPD, (unsigned)per_slot)) return;
+  const double x2 = ordered_sum(S.partials, per_slot, 1, red);
   if (threadIdx.x == 0) {
-    *a.ticket = 0;
-    minres_after_update(a.st, x2);
+    S.tickets[TK_UPD] = 0;
+    minres_after_update(S.st, x2);
   }
 }
 
@@ -309,101 +378,204 @@ __device__ __forceinline__ void load_table(cplx<T> *dst, const cplx<T> *src, int
   for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
 }
 
-// zfwd: blockIdx.x covers g.lz consecutive (x,y) lines.  TF is the storage type of the
-// input fields (TF = T except when a double-precision transform reads float fields).
+// Block-uniform "skip this item": a Krylov item of a slot whose solve is done.
+template <typename TF, int PRO> __device__ __forceinline__ bool skip_item(const SlotDev<TF> &S) {
+  if constexpr (PRO_IS_KRYLOV(PRO)) return block_read_flag(&S.st->done) != 0;
+  return false;
+}
+
+// Per-point epilogue of the inverse passes: r[] is the transformed value of the owned
+// components c0 .. c0 + NC - 1 at point v; accumulates the slot's reduction terms.
+template <typename T, typename TF, int EPI, int NC>
+__device__ __forceinline__ void epilogue_point(const SlotDev<TF> &S, const ExtIO<TF> &io,
+                                               const KRoles<TF> &kr, T c1, long long V,
+                                               long long v, int c0, const T *r, const TF *r1v,
+                                               const TF *r2v, double &acc0, double &acc1,
+                                               double &acc2) {
+#pragma unroll
+  for (int q = 0; q < NC; ++q) {
+    const long long i = (long long)(c0 + q) * V + v;
+    if constexpr (EPI == EPI_STORE) {
+      io.out[i] = (TF)r[q];
+    } else if constexpr (EPI == EPI_RESIDUAL) {
+      S.b[i] = (TF)r[q];
+      acc0 = fmax(acc0, fabs((double)r[q]));
+    } else if constexpr (EPI == EPI_REPROJECT) {
+      const TF x = (TF)r[q];
+      kr.X[i] = x;
+      S.eps[i] += x;
+      S.dfl[i] += x;
+    } else {
+      const T y = r[q] - c1 * (T)r1v[q];
+      kr.Y[i] = (TF)y;
+      acc0 += (double)r2v[q] * (double)y;
+      acc1 += (double)y * (double)y;
+      acc2 += (double)r2v[q] * (double)r2v[q];
+    }
+  }
+}
+
+// End of an inverse item: the slot's max |b| (residual) or its three MINRES dot products,
+// finished by the slot's last item.
+template <typename TF, int EPI>
+__device__ __forceinline__ void finish_inverse(const SlotDev<TF> &S, double acc0, double acc1,
+                                               double acc2, int local, int per_slot,
+                                               double *red) {
+  if constexpr (EPI == EPI_RESIDUAL) {
+    const double part = block_max(acc0, red);
+    if (threadIdx.x == 0) S.partials[local] = part;
+  } else if constexpr (EPI == EPI_MINRES) {
+    const double q0 = block_sum(acc0, red);
+    const double q1 = block_sum(acc1, red);
+    const double q2 = block_sum(acc2, red);
+    if (threadIdx.x == 0) {
+      S.partials[3 * local] = q0;
+      S.partials[3 * local + 1] = q1;
+      S.partials[3 * local + 2] = q2;
+    }
+  } else {
+    return;
+  }
+  if (!last_item_arrives(S.tickets + TK_ZINV, (unsigned)per_slot)) return;
+  if constexpr (EPI == EPI_RESIDUAL) {
+    const double m = ordered_max(S.partials, per_slot, 1, red);
+    if (threadIdx.x == 0) {
+      S.results[40] = m;
+      S.tickets[TK_ZINV] = 0;
+    }
+  } else {
+    const double d0 = ordered_sum(S.partials, per_slot, 3, red);
+    const double d1 = ordered_sum(S.partials + 1, per_slot, 3, red);
+    const double d2 = ordered_sum(S.partials + 2, per_slot, 3, red);
+    if (threadIdx.x == 0) {
+      minres_after_matvec(S.st, d0, d1, d2);
+      S.tickets[TK_ZINV] = 0;
+    }
+  }
+}
+
+// ---- five-pass kernels ------------------------------------------------------------------
+
 // z kernels: three blocks per SM in float (80 registers), two in double
 #define Z_MIN_BLOCKS(T) (sizeof(T) == 4 ? 3 : 2)
 
+// zfwd: an item is (slot, tile of g.lz consecutive (x,y) lines).  TF is the storage type of
+// the fields (TF = T except when a double-precision transform reads float fields).
 template <typename T, typename TF, int PRO>
 __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
-    zfwd_kernel(Grid<T> g, ProArgs<TF> a, cplx<T> *__restrict__ spec) {
-  if (PRO >= PRO_TANGENT_TABLE && a.st->done) return;
+    zfwd_kernel(Grid<T> g, const SlotDev<TF> *__restrict__ tab, SlotList list, ExtIO<TF> io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int nz = g.nz, hz = g.hz;
+  __shared__ double red[32];
+  __shared__ __align__(16) unsigned char sdesc[sizeof(SlotDev<TF>)];
+  const int nz = g.nz, hs = g.hs;
+  const long long V = g.V;
   const long long nlines_all = (long long)g.nx * g.ny;
-  const long long line0 = (long long)blockIdx.x * g.lz;
-  const int nl = (int)min((long long)g.lz, nlines_all - line0);
-  const int ti = (nl == g.lz) ? 0 : 1;
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *bufB = bufA + zbuf_elems(g.lz, nz);
   cplx<T> *tw = bufB + zbuf_elems(g.lz, nz);
   load_table<T>(tw, g.twz, nz);
-  PendingUpdate<T> u{};
-  if constexpr (PRO >= PRO_TANGENT_TABLE) u = pending_update<T>(a);
-  double xx = 0.0;
-  for (int e = threadIdx.x; e < nl * nz; e += blockDim.x) {
-    const int l = udiv(e, g.fd_nz), z = e - l * nz;
-    const long long v = (line0 + l) * nz + z;
-    T tau[6];
-    if constexpr (PRO >= PRO_TANGENT_TABLE)
-      tangent_prologue<T, TF, PRO, true>(g, a, v, u, 0, tau, xx);
-    else
-      prologue<T, TF, PRO>(g, a, v, (T)1, tau);
+  const int per = items_z(g);
+  const int n_items = list_items(list, per);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int k = udiv(item, g.fd_it_z);
+    const int local = item - k * per;
+    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc);
+    if (skip_item<TF, PRO>(S)) continue;
+    const long long line0 = (long long)local * g.lz;
+    const int nl = (int)min((long long)g.lz, nlines_all - line0);
+    const int ti = (nl == g.lz) ? 0 : 1;
+    KrylovIn<T, TF> u{};
+    if constexpr (PRO_IS_KRYLOV(PRO)) u = krylov_in<T, TF>(S);
+    double xx = 0.0;
+    __syncthreads();  // table loaded; previous item done with the buffers
+    for (int e = threadIdx.x; e < nl * nz; e += blockDim.x) {
+      const int l = udiv(e, g.fd_nz), z = e - l * nz;
+      const long long v = (line0 + l) * nz + z;
+      T tau[6];
+      if constexpr (PRO_IS_KRYLOV(PRO))
+        tangent_prologue<T, TF, PRO, true>(S, V, v, u, 0, tau, xx);
+      else
+        prologue<T, TF, PRO>(S, io.in, V, v, tau);
 #pragma unroll
-    for (int p = 0; p < 3; ++p)
-      bufA[sidx<true>((p * nl + l) * nz + z)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
-  }
-  __syncthreads();
-  const LineLayout L(3 * nl, 3 * nl, 0, nz, 1, g.fd_z3[ti], g.fd_z3[ti]);
-  cplx<T> *res = smem_fft<T, false, false, true>(bufA, bufB, L, g.pz, tw);
-  // split the paired transform: A = (Z_k + conj Z_{-k}) / 2, B = (Z_k - conj Z_{-k}) / 2i
-  for (int e = threadIdx.x; e < 3 * nl * hz; e += blockDim.x) {
-    const int p = udiv(e, g.fd_znh[ti]);
-    const int rem = e - p * nl * hz;
-    const int l = udiv(rem, g.fd_hz), k = rem - l * hz;
-    const cplx<T> Z = res[sidx<true>((p * nl + l) * nz + k)];
-    const int km = (k == 0) ? 0 : nz - k;
-    const cplx<T> Zm = res[sidx<true>((p * nl + l) * nz + km)];
-    const cplx<T> A = mk<T>((T)0.5 * (Z.x + Zm.x), (T)0.5 * (Z.y - Zm.y));
-    const cplx<T> B = mk<T>((T)0.5 * (Z.y + Zm.y), (T)0.5 * (Zm.x - Z.x));
-    const long long off = (line0 + l) * hz + k;
-    spec[(2 * p) * g.S + off] = A;
-    spec[(2 * p + 1) * g.S + off] = B;
-  }
-  if constexpr (PRO >= PRO_TANGENT_TABLE) {
-    __shared__ double red[32];
-    if (u.on) finish_pending_update(a, xx, blockIdx.x, gridDim.x, red);
+      for (int p = 0; p < 3; ++p)
+        bufA[sidx<true>((p * nl + l) * nz + z)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
+    }
+    __syncthreads();
+    const LineLayout L(3 * nl, 3 * nl, 0, nz, 1, g.fd_z3[ti], g.fd_z3[ti]);
+    cplx<T> *res = smem_fft<T, false, false, true>(bufA, bufB, L, g.pz, tw);
+    cplx<T> *spec = reinterpret_cast<cplx<T> *>(S.spec);
+    // split the paired transform: A = (Z_k + conj Z_{-k}) / 2, B = (Z_k - conj Z_{-k}) / 2i
+    for (int e = threadIdx.x; e < 3 * nl * hs; e += blockDim.x) {
+      const int p = udiv(e, g.fd_znh[ti]);
+      const int rem = e - p * nl * hs;
+      const int l = udiv(rem, g.fd_hs), kk = rem - l * hs;
+      const cplx<T> Z = res[sidx<true>((p * nl + l) * nz + kk)];
+      const int km = (kk == 0) ? 0 : nz - kk;
+      const cplx<T> Zm = res[sidx<true>((p * nl + l) * nz + km)];
+      const cplx<T> A = mk<T>((T)0.5 * (Z.x + Zm.x), (T)0.5 * (Z.y - Zm.y));
+      const cplx<T> B = mk<T>((T)0.5 * (Z.y + Zm.y), (T)0.5 * (Zm.x - Z.x));
+      const long long off = (line0 + l) * hs + kk;
+      spec[(2 * p) * g.S + off] = A;
+      spec[(2 * p + 1) * g.S + off] = B;
+    }
+    if constexpr (PRO_IS_KRYLOV(PRO)) {
+      if (u.on) finish_pending_update(S, xx, local, per, red);
+    }
+    __syncthreads();
   }
 }
 
-// y passes: grid (ceil(hz/ky), nx, 6); lines are kz columns of one (c, x) slab.
-template <typename T, bool INV>
+// y passes: an item is (slot, kz column tile, x, component); lines are kz columns of one
+// (c, x) slab.
+template <typename T, typename TF, bool INV, bool KRY>
 __global__ void __launch_bounds__(SSFFT_THREADS)
-    ypass_kernel(Grid<T> g, cplx<T> *__restrict__ spec, const MinresState *st) {
-  if (st && st->done) return;
+    ypass_kernel(Grid<T> g, const SlotDev<TF> *__restrict__ tab, SlotList list) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int ny = g.ny, hz = g.hz;
-  const int k0 = blockIdx.x * g.ky;
-  const int nk = min(g.ky, hz - k0);
-  const int ti = (nk == g.ky) ? 0 : 1;
-  const int x = blockIdx.y, c = blockIdx.z;
+  const int ny = g.ny, hs = g.hs;
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *bufB = bufA + g.ky * ny;
   cplx<T> *tw = bufB + g.ky * ny;
   load_table<T>(tw, g.twy, ny);
-  cplx<T> *base = spec + c * g.S + (long long)x * ny * hz + k0;
-  for (int e = threadIdx.x; e < ny * nk; e += blockDim.x) {
-    const int y = udiv(e, g.fd_ky[ti]), kk = e - y * nk;
-    bufA[y * nk + kk] = base[(long long)y * hz + kk];
-  }
-  __syncthreads();
-  const LineLayout L(nk, nk, 0, 1, nk, g.fd_ky[ti], g.fd_ky[ti]);
-  cplx<T> *res = smem_fft<T, INV, true>(bufA, bufB, L, g.py, tw);
-  for (int e = threadIdx.x; e < ny * nk; e += blockDim.x) {
-    const int y = udiv(e, g.fd_ky[ti]), kk = e - y * nk;
-    base[(long long)y * hz + kk] = res[y * nk + kk];
+  const int per = items_y(g);
+  const int n_items = list_items(list, per);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int k = udiv(item, g.fd_it_y);
+    const int local = item - k * per;
+    const SlotDev<TF> &S = tab[list.ids[k]];
+    if (KRY && block_read_flag(&S.st->done)) continue;
+    const int c = udiv(local, g.fd_nkynx);
+    const int r1 = local - c * g.nky * g.nx;
+    const int x = udiv(r1, g.fd_nky);
+    const int kb = r1 - x * g.nky;
+    const int k0 = kb * g.ky;
+    const int nk = min(g.ky, hs - k0);
+    const int ti = (nk == g.ky) ? 0 : 1;
+    cplx<T> *base = reinterpret_cast<cplx<T> *>(S.spec) + c * g.S + (long long)x * ny * hs + k0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < ny * nk; e += blockDim.x) {
+      const int y = udiv(e, g.fd_ky[ti]), kk = e - y * nk;
+      bufA[y * nk + kk] = base[(long long)y * hs + kk];
+    }
+    __syncthreads();
+    const LineLayout L(nk, nk, 0, 1, nk, g.fd_ky[ti], g.fd_ky[ti]);
+    cplx<T> *res = smem_fft<T, INV, true>(bufA, bufB, L, g.py, tw);
+    for (int e = threadIdx.x; e < ny * nk; e += blockDim.x) {
+      const int y = udiv(e, g.fd_ky[ti]), kk = e - y * nk;
+      base[(long long)y * hs + kk] = res[y * nk + kk];
+    }
+    __syncthreads();
   }
 }
 
 // Gamma-hat : tau-hat at one frequency, in place on the six complex components.
 template <typename T>
-__device__ __forceinline__ void green_apply(const Grid<T> &g, int kx, int ky, int kz,
-                                            cplx<T> *m) {
+__device__ __forceinline__ void green_apply(const Grid<T> &g, const double *mask, int kx, int ky,
+                                            int kz, cplx<T> *m) {
   const bool nyq = ((g.nx % 2 == 0) && kx == g.nx / 2) || ((g.ny % 2 == 0) && ky == g.ny / 2) ||
                    ((g.nz % 2 == 0) && kz == g.nz / 2);
   if (kx == 0 && ky == 0 && kz == 0) {
 #pragma unroll
-    for (int c = 0; c < 6; ++c) m[c] = cscale<T>(m[c], g.mask[c] * g.scale);
+    for (int c = 0; c < 6; ++c) m[c] = cscale<T>(m[c], (T)mask[c] * g.scale);
     return;
   }
   if (nyq) {
@@ -439,100 +611,61 @@ __device__ __forceinline__ void green_apply(const Grid<T> &g, int kx, int ky, in
                sc * r2 * (t0 * u1.y + u0.y * t1 - tu.y * t0 * t1));
 }
 
-// x pass: grid (ceil(hz/kx), ny); forward x-FFT of all six components, Gamma-hat,
-// inverse x-FFT, store.
+// x pass: an item is (slot, y, kz column tile); forward x-FFT of all six components,
+// Gamma-hat, inverse x-FFT, store.  KRY: skip slots whose solve is done.
 #define XPASS_THREADS SSFFT_THREADS
-template <typename T>
+template <typename T, typename TF, bool KRY>
 __global__ void __launch_bounds__(XPASS_THREADS)
-    xpass_kernel(Grid<T> g, cplx<T> *__restrict__ spec, const MinresState *st) {
-  if (st && st->done) return;
+    xpass_kernel(Grid<T> g, const SlotDev<TF> *__restrict__ tab, SlotList list) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int nx = g.nx, ny = g.ny, hz = g.hz;
-  const int k0 = blockIdx.x * g.kx;
-  const int nk = min(g.kx, hz - k0);
-  const int ti = (nk == g.kx) ? 0 : 1;
-  const int y = blockIdx.y;
-  const int slab = nx * nk;                      // live elements per component
+  const int nx = g.nx, ny = g.ny, hs = g.hs;
   const int sst = xslab_elems<T>(nx, g.kx);      // padded slab stride
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *bufB = bufA + 6 * sst;
   cplx<T> *tw = bufB + 6 * sst;
   load_table<T>(tw, g.twx, nx);
-  for (int e = threadIdx.x; e < 6 * slab; e += blockDim.x) {
-    const int c = udiv(e, g.fd_xslab[ti]), rem = e - c * slab;
-    const int x = udiv(rem, g.fd_kx[ti]), kk = rem - x * nk;
-    bufA[c * sst + x * nk + kk] = spec[c * g.S + ((long long)x * ny + y) * hz + k0 + kk];
-  }
-  __syncthreads();
-  const LineLayout L(6 * nk, nk, sst, 1, nk, g.fd_x6k[ti], g.fd_kx[ti]);
-  cplx<T> *res = smem_fft<T, false, true>(bufA, bufB, L, g.px, tw);
-  cplx<T> *other = (res == bufA) ? bufB : bufA;
-  for (int e = threadIdx.x; e < slab; e += blockDim.x) {
-    const int x = udiv(e, g.fd_kx[ti]), kk = e - x * nk;
-    cplx<T> m[6];
+  const int per = items_x(g);
+  const int n_items = list_items(list, per);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int kk_slot = udiv(item, g.fd_it_x);
+    const int local = item - kk_slot * per;
+    const SlotDev<TF> &S = tab[list.ids[kk_slot]];
+    if (KRY && block_read_flag(&S.st->done)) continue;
+    const int y = udiv(local, g.fd_nkx);
+    const int kb = local - y * g.nkx;
+    const int k0 = kb * g.kx;
+    const int nk = min(g.kx, hs - k0);
+    const int ti = (nk == g.kx) ? 0 : 1;
+    const int slab = nx * nk;                      // live elements per component
+    cplx<T> *spec = reinterpret_cast<cplx<T> *>(S.spec);
+    __syncthreads();
+    for (int e = threadIdx.x; e < 6 * slab; e += blockDim.x) {
+      const int c = udiv(e, g.fd_xslab[ti]), rem = e - c * slab;
+      const int x = udiv(rem, g.fd_kx[ti]), kk = rem - x * nk;
+      bufA[c * sst + x * nk + kk] = spec[c * g.S + ((long long)x * ny + y) * hs + k0 + kk];
+    }
+    __syncthreads();
+    const LineLayout L(6 * nk, nk, sst, 1, nk, g.fd_x6k[ti], g.fd_kx[ti]);
+    cplx<T> *res = smem_fft<T, false, true>(bufA, bufB, L, g.px, tw);
+    cplx<T> *other = (res == bufA) ? bufB : bufA;
+    for (int e = threadIdx.x; e < slab; e += blockDim.x) {
+      const int x = udiv(e, g.fd_kx[ti]), kk = e - x * nk;
+      cplx<T> m[6];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) m[c] = res[c * sst + x * nk + kk];
-    green_apply<T>(g, x, y, k0 + kk, m);
+      for (int c = 0; c < 6; ++c) m[c] = res[c * sst + x * nk + kk];
+      green_apply<T>(g, S.mask, x, y, k0 + kk, m);
 #pragma unroll
-    for (int c = 0; c < 6; ++c) res[c * sst + x * nk + kk] = m[c];
+      for (int c = 0; c < 6; ++c) res[c * sst + x * nk + kk] = m[c];
+    }
+    __syncthreads();
+    cplx<T> *out = smem_fft<T, true, true>(res, other, L, g.px, tw);
+    for (int e = threadIdx.x; e < 6 * slab; e += blockDim.x) {
+      const int c = udiv(e, g.fd_xslab[ti]), rem = e - c * slab;
+      const int x = udiv(rem, g.fd_kx[ti]), kk = rem - x * nk;
+      spec[c * g.S + ((long long)x * ny + y) * hs + k0 + kk] = out[c * sst + x * nk + kk];
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  cplx<T> *out = smem_fft<T, true, true>(res, other, L, g.px, tw);
-  for (int e = threadIdx.x; e < 6 * slab; e += blockDim.x) {
-    const int c = udiv(e, g.fd_xslab[ti]), rem = e - c * slab;
-    const int x = udiv(rem, g.fd_kx[ti]), kk = rem - x * nk;
-    spec[c * g.S + ((long long)x * ny + y) * hz + k0 + kk] = out[c * sst + x * nk + kk];
-  }
-}
-
-// ---- epilogue modes of zinv ----------------------------------------------------------
-enum { EPI_STORE = 0, EPI_RESIDUAL = 1, EPI_MINRES = 2 };
-
-template <typename T> struct EpiArgs {
-  T *out;                 // STORE/RESIDUAL: output planes; MINRES: y'
-  const T *r1;            // MINRES: previous Lanczos vector u_{j-1}
-  const T *r2;            // MINRES: current Lanczos vector u_j (v = s * u_j)
-  MinresState *st;        // MINRES
-  double *partials;       // per-block partial results
-  unsigned int *ticket;   // last-block counter
-  double *result;         // RESIDUAL: max |b|
-};
-
-// MINRES scalar recurrence after the matvec (Paige & Saunders 1975; scipy's minres loop
-// body up to the plane rotation).  d0 = r2 . y', d1 = y' . y', d2 = r2 . r2 where
-// y' = A v - (beta/oldb) r1 and v = r2 / beta.  The orthogonalised y'' = y' - (alfa/beta) r2
-// is formed by the next kernel; its norm follows from the three dot products:
-// |y''|^2 = d1 - 2 c d0 + c^2 d2 with c = alfa / beta.
-static __device__ __noinline__ void minres_after_matvec(MinresState *st, double d0, double d1,
-                                                 double d2) {
-  MinresState s = *st;
-  s.itn += 1;
-  s.alfa = s.s * d0;
-  s.coef = s.alfa / s.beta;
-  double beta2 = d1 - 2.0 * s.coef * d0 + s.coef * s.coef * d2;
-  if (beta2 < 0.0) beta2 = 0.0;
-  s.oldb = s.beta;
-  s.beta = sqrt(beta2);
-  s.tnorm2 += s.alfa * s.alfa + s.oldb * s.oldb + s.beta * s.beta;
-  if (s.itn == 1 && s.beta / s.beta1 <= 10.0 * s.eps) s.istop = -1;
-  s.oldeps = s.epsln;
-  s.delta = s.cs * s.dbar + s.sn * s.alfa;
-  const double gbar = s.sn * s.dbar - s.cs * s.alfa;
-  s.epsln = s.sn * s.beta;
-  s.dbar = -s.cs * s.beta;
-  s.root = hypot(gbar, s.dbar);
-  s.gamma = fmax(hypot(gbar, s.beta), s.eps);
-  s.cs = gbar / s.gamma;
-  s.sn = s.beta / s.gamma;
-  s.phi = s.cs * s.phibar;
-  s.phibar = s.sn * s.phibar;
-  s.denom = 1.0 / s.gamma;
-  s.gmax = fmax(s.gmax, s.gamma);
-  s.gmin = fmin(s.gmin, s.gamma);
-  s.s_prev = s.s;
-  s.s = (s.beta > 0.0) ? 1.0 / s.beta : 0.0;
-  s.c_r1 = (s.oldb > 0.0) ? s.beta / s.oldb : 0.0;
-  *st = s;
 }
 
 #define ZINV_PREFETCH 3  // epilogue elements per thread whose r1/r2 are loaded early
@@ -540,145 +673,116 @@ static __device__ __noinline__ void minres_after_matvec(MinresState *st, double 
 
 template <typename T, typename TF, int EPI>
 __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
-    zinv_kernel(Grid<T> g, EpiArgs<TF> a, const cplx<T> *__restrict__ spec) {
-  if (EPI == EPI_MINRES && a.st->done) return;
+    zinv_kernel(Grid<T> g, const SlotDev<TF> *__restrict__ tab, SlotList list, ExtIO<TF> io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[32];
+  __shared__ __align__(16) unsigned char sdesc[sizeof(SlotDev<TF>)];
   const int nz = g.nz, hz = g.hz;
+  const long long V = g.V;
   const long long nlines_all = (long long)g.nx * g.ny;
-  const long long line0 = (long long)blockIdx.x * g.lz;
-  const int nl = (int)min((long long)g.lz, nlines_all - line0);
-  const int ti = (nl == g.lz) ? 0 : 1;
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *bufB = bufA + zbuf_elems(g.lz, nz);
   cplx<T> *tw = bufB + zbuf_elems(g.lz, nz);
   load_table<T>(tw, g.twz, nz);
-  const int nel = nl * nz;
-  // MINRES: issue the loads of r1 and r2 for this thread's first elements before the
-  // transform so that their latency overlaps it
-  TF p1[EPI == EPI_MINRES ? ZINV_PREFETCH : 1][6], p2[EPI == EPI_MINRES ? ZINV_PREFETCH : 1][6];
-  const bool prefetch = (EPI == EPI_MINRES) && nel <= ZINV_PREFETCH * (int)blockDim.x;
-  if (EPI == EPI_MINRES && prefetch) {
+  const int per = items_z(g);
+  const int n_items = list_items(list, per);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int k = udiv(item, g.fd_it_z);
+    const int local = item - k * per;
+    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc);
+    if (EPI == EPI_MINRES && block_read_flag(&S.st->done)) continue;
+    const long long line0 = (long long)local * g.lz;
+    const int nl = (int)min((long long)g.lz, nlines_all - line0);
+    const int ti = (nl == g.lz) ? 0 : 1;
+    const int nel = nl * nz;
+    KRoles<TF> kr{};
+    T c1 = 0;
+    if constexpr (EPI == EPI_MINRES) {
+      kr = kroles<TF>(S, S.st->itn);
+      c1 = (T)S.st->c_r1;
+    } else if constexpr (EPI == EPI_REPROJECT) {
+      kr = kroles<TF>(S, 0);
+    }
+    // MINRES: issue the loads of r1 and r2 for this thread's first elements before the
+    // transform so that their latency overlaps it
+    TF p1[EPI == EPI_MINRES ? ZINV_PREFETCH : 1][6], p2[EPI == EPI_MINRES ? ZINV_PREFETCH : 1][6];
+    const bool prefetch = (EPI == EPI_MINRES) && nel <= ZINV_PREFETCH * (int)blockDim.x;
+    if (EPI == EPI_MINRES && prefetch) {
 #pragma unroll
-    for (int i = 0; i < ZINV_PREFETCH; ++i) {
-      const int e = threadIdx.x + i * blockDim.x;
-      if (e < nel) {
-        const long long v = line0 * nz + e;
+      for (int i = 0; i < ZINV_PREFETCH; ++i) {
+        const int e = threadIdx.x + i * blockDim.x;
+        if (e < nel) {
+          const long long v = line0 * nz + e;
 #pragma unroll
-        for (int c = 0; c < 6; ++c) {
-          p1[i][c] = a.r1[c * g.V + v];
-          p2[i][c] = a.r2[c * g.V + v];
+          for (int c = 0; c < 6; ++c) {
+            p1[i][c] = kr.P[c * V + v];
+            p2[i][c] = kr.Q[c * V + v];
+          }
         }
       }
     }
-  }
-  // rebuild the full z spectrum of Z = A + iB from the stored half (Hermitian in z)
-  for (int e = threadIdx.x; e < 3 * nel; e += blockDim.x) {
-    const int p = udiv(e, g.fd_znz[ti]);
-    const int rem = e - p * nel;
-    const int l = udiv(rem, g.fd_nz), k = rem - l * nz;
-    const bool low = (k < hz);
-    const int ks = low ? k : nz - k;
-    const long long off = (line0 + l) * hz + ks;
-    const cplx<T> A = spec[(2 * p) * g.S + off];
-    const cplx<T> B = spec[(2 * p + 1) * g.S + off];
-    bufA[sidx<true>((p * nl + l) * nz + k)] =
-        low ? mk<T>(A.x - B.y, A.y + B.x) : mk<T>(A.x + B.y, B.x - A.y);
-  }
-  __syncthreads();
-  const LineLayout L(3 * nl, 3 * nl, 0, nz, 1, g.fd_z3[ti], g.fd_z3[ti]);
-  cplx<T> *res = smem_fft<T, true, false, true>(bufA, bufB, L, g.pz, tw);
-  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-  T c1 = 0;
-  if (EPI == EPI_MINRES) c1 = (T)a.st->c_r1;
-  // per-element epilogue; for MINRES r1v / r2v hold r1 and r2 at this point
-  auto finish = [&](int e, const TF *r1v, const TF *r2v) {
-    const long long v = line0 * nz + e;
-    T r[6];
-#pragma unroll
-    for (int p = 0; p < 3; ++p) {
-      const cplx<T> Z = res[sidx<true>(p * nel + e)];
-      r[2 * p] = Z.x;
-      r[2 * p + 1] = Z.y;
+    const cplx<T> *spec = reinterpret_cast<const cplx<T> *>(S.spec);
+    __syncthreads();
+    // rebuild the full z spectrum of Z = A + iB from the stored half (Hermitian in z)
+    for (int e = threadIdx.x; e < 3 * nel; e += blockDim.x) {
+      const int p = udiv(e, g.fd_znz[ti]);
+      const int rem = e - p * nel;
+      const int l = udiv(rem, g.fd_nz), kk = rem - l * nz;
+      const bool low = (kk < hz);
+      const int ks = low ? kk : nz - kk;
+      const long long off = (line0 + l) * g.hs + ks;
+      const bool nyq = 2 * ks == nz;  // the unstored Nyquist column is zero
+      const cplx<T> A = nyq ? mk<T>((T)0, (T)0) : spec[(2 * p) * g.S + off];
+      const cplx<T> B = nyq ? mk<T>((T)0, (T)0) : spec[(2 * p + 1) * g.S + off];
+      bufA[sidx<true>((p * nl + l) * nz + kk)] =
+          low ? mk<T>(A.x - B.y, A.y + B.x) : mk<T>(A.x + B.y, B.x - A.y);
     }
-    if (EPI == EPI_STORE) {
+    __syncthreads();
+    const LineLayout L(3 * nl, 3 * nl, 0, nz, 1, g.fd_z3[ti], g.fd_z3[ti]);
+    cplx<T> *res = smem_fft<T, true, false, true>(bufA, bufB, L, g.pz, tw);
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+    auto finish = [&](int e, const TF *r1v, const TF *r2v) {
+      const long long v = line0 * nz + e;
+      T r[6];
 #pragma unroll
-      for (int c = 0; c < 6; ++c) a.out[c * g.V + v] = (TF)r[c];
-    } else if (EPI == EPI_RESIDUAL) {
+      for (int p = 0; p < 3; ++p) {
+        const cplx<T> Z = res[sidx<true>(p * nel + e)];
+        r[2 * p] = Z.x;
+        r[2 * p + 1] = Z.y;
+      }
+      epilogue_point<T, TF, EPI, 6>(S, io, kr, c1, V, v, 0, r, r1v, r2v, acc0, acc1, acc2);
+    };
+    if (EPI == EPI_MINRES && prefetch) {
 #pragma unroll
-      for (int c = 0; c < 6; ++c) {
-        a.out[c * g.V + v] = (TF)r[c];
-        acc0 = fmax(acc0, fabs((double)r[c]));
+      for (int i = 0; i < ZINV_PREFETCH; ++i) {
+        const int e = threadIdx.x + i * blockDim.x;
+        if (e < nel) finish(e, p1[i], p2[i]);
       }
     } else {
+      for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+        TF q1[6], q2[6];
+        if (EPI == EPI_MINRES) {
+          const long long v = line0 * nz + e;
 #pragma unroll
-      for (int c = 0; c < 6; ++c) {
-        const T y = r[c] - c1 * (T)r1v[c];
-        a.out[c * g.V + v] = (TF)y;
-        acc0 += (double)r2v[c] * (double)y;
-        acc1 += (double)y * (double)y;
-        acc2 += (double)r2v[c] * (double)r2v[c];
-      }
-    }
-  };
-  if (EPI == EPI_MINRES && prefetch) {
-#pragma unroll
-    for (int i = 0; i < ZINV_PREFETCH; ++i) {
-      const int e = threadIdx.x + i * blockDim.x;
-      if (e < nel) finish(e, p1[i], p2[i]);
-    }
-  } else {
-    for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-      TF q1[6], q2[6];
-      if (EPI == EPI_MINRES) {
-        const long long v = line0 * nz + e;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) {
-          q1[c] = a.r1[c * g.V + v];
-          q2[c] = a.r2[c * g.V + v];
+          for (int c = 0; c < 6; ++c) {
+            q1[c] = kr.P[c * V + v];
+            q2[c] = kr.Q[c * V + v];
+          }
         }
+        finish(e, q1, q2);
       }
-      finish(e, q1, q2);
     }
-  }
-  if (EPI == EPI_STORE) return;
-  if (EPI == EPI_RESIDUAL) {
-    const double part = block_max(acc0, red);
-    if (threadIdx.x == 0) a.partials[blockIdx.x] = part;
-  } else {
-    const double q0 = block_sum(acc0, red);
-    const double q1 = block_sum(acc1, red);
-    const double q2 = block_sum(acc2, red);
-    if (threadIdx.x == 0) {
-      a.partials[3 * blockIdx.x] = q0;
-      a.partials[3 * blockIdx.x + 1] = q1;
-      a.partials[3 * blockIdx.x + 2] = q2;
-    }
-  }
-  if (!last_block_arrives(a.ticket)) return;
-  if (EPI == EPI_RESIDUAL) {
-    const double m = ordered_max(a.partials, gridDim.x, 1, red);
-    if (threadIdx.x == 0) {
-      *a.result = m;
-      *a.ticket = 0;
-    }
-  } else {
-    const double d0 = ordered_sum(a.partials, gridDim.x, 3, red);
-    const double d1 = ordered_sum(a.partials + 1, gridDim.x, 3, red);
-    const double d2 = ordered_sum(a.partials + 2, gridDim.x, 3, red);
-    if (threadIdx.x == 0) {
-      minres_after_matvec(a.st, d0, d1, d2);
-      *a.ticket = 0;
-    }
+    finish_inverse<TF, EPI>(S, acc0, acc1, acc2, local, per, red);
+    __syncthreads();
   }
 }
 
 // ---- plane-fused passes (grids whose yz planes fit in shared memory) -------------------
 //
-// zyfwd: one block per (x plane, component pair p): tau of the pair over the whole plane
-// (prologue), real-to-complex along z, complex FFT along y, write the half spectrum of
-// both components.  yzinv is its inverse followed by the epilogue.  With xpass in between
-// a projection is three passes and the spectrum crosses HBM four times instead of eight.
+// zyfwd: an item is (slot, x plane, component pair p): tau of the pair over the whole
+// plane (prologue), real-to-complex along z, complex FFT along y, write the half spectrum
+// of both components.  yzinv is its inverse followed by the epilogue.  The three pair
+// items of one plane are adjacent, so the Krylov vectors all three read come from L2.
 
 // Shared memory of the plane passes: two buffers of the padded plane (ny (nz + 2)
 // complex, enough for the paired z lines and for the split half spectra of two
@@ -693,11 +797,12 @@ template <typename T> inline size_t smem_plane_bytes(int ny, int nz) {
 
 template <typename T, typename TF, int PRO, int PT>
 __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
-    zyfwd_kernel(Grid<T> g, ProArgs<TF> a, cplx<T> *__restrict__ spec) {
-  if (PRO >= PRO_TANGENT_TABLE && a.st->done) return;
+    zyfwd_kernel(Grid<T> g, const SlotDev<TF> *__restrict__ tab, SlotList list, ExtIO<TF> io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int ny = g.ny, nz = g.nz, hz = g.hz;
-  const int x = blockIdx.x, p = blockIdx.y;
+  __shared__ double red[32];
+  __shared__ __align__(16) unsigned char sdesc[sizeof(SlotDev<TF>)];
+  const int ny = g.ny, nz = g.nz, hs = g.hs;
+  const long long V = g.V;
   const int cap = padded_len(ny * (nz + 2));
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *bufB = bufA + cap;
@@ -705,55 +810,67 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
   cplx<T> *twz = twy + ny;
   load_table<T>(twy, g.twy, ny);
   load_table<T>(twz, g.twz, nz);
-  PendingUpdate<T> u{};
-  if constexpr (PRO >= PRO_TANGENT_TABLE) u = pending_update<T>(a);
-  double xx = 0.0;
-  const long long vbase = (long long)x * ny * nz;
-  for (int e = threadIdx.x; e < ny * nz; e += blockDim.x) {
-    T tau[6];
-    if constexpr (PRO >= PRO_TANGENT_TABLE) {
-      tangent_prologue<T, TF, PRO, false>(g, a, vbase + e, u, p, tau, xx);
-      bufA[sidx<true>(e)] = mk<T>(tau[0], tau[1]);
-    } else {
-      prologue<T, TF, PRO>(g, a, vbase + e, (T)1, tau);
-      bufA[sidx<true>(e)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
+  const int per = items_plane(g);
+  const int n_items = list_items(list, per);
+  const int plane = ny * hs;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int k = udiv(item, g.fd_it_plane);
+    const int local = item - k * per;
+    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc);
+    if (skip_item<TF, PRO>(S)) continue;
+    const int x = udiv(local, g.fd_3);
+    const int p = local - 3 * x;
+    KrylovIn<T, TF> u{};
+    if constexpr (PRO_IS_KRYLOV(PRO)) u = krylov_in<T, TF>(S);
+    double xx = 0.0;
+    const long long vbase = (long long)x * ny * nz;
+    __syncthreads();
+    for (int e = threadIdx.x; e < ny * nz; e += blockDim.x) {
+      T tau[6];
+      if constexpr (PRO_IS_KRYLOV(PRO)) {
+        tangent_prologue<T, TF, PRO, false>(S, V, vbase + e, u, p, tau, xx);
+        bufA[sidx<true>(e)] = mk<T>(tau[0], tau[1]);
+      } else {
+        prologue<T, TF, PRO>(S, io.in, V, vbase + e, tau);
+        bufA[sidx<true>(e)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
+      }
     }
-  }
-  __syncthreads();
-  const LineLayout Lz(ny, ny, 0, nz, 1, g.fd_ny, g.fd_ny);
-  cplx<T> *res = smem_fft<T, false, false, true>(bufA, bufB, Lz, g.pz, twz);
-  cplx<T> *oth = (res == bufA) ? bufB : bufA;
-  // split the paired transform into the half spectra of components 2p and 2p+1,
-  // laid out [c][y][k] for the y transform
-  const int plane = ny * hz;
-  for (int e = threadIdx.x; e < plane; e += blockDim.x) {
-    const int y = udiv(e, g.fd_hz), k = e - y * hz;
-    const cplx<T> Z = res[sidx<true>(y * nz + k)];
-    const cplx<T> Zm = res[sidx<true>(y * nz + (k == 0 ? 0 : nz - k))];
-    oth[e] = mk<T>((T)0.5 * (Z.x + Zm.x), (T)0.5 * (Z.y - Zm.y));
-    oth[plane + e] = mk<T>((T)0.5 * (Z.y + Zm.y), (T)0.5 * (Zm.x - Z.x));
-  }
-  __syncthreads();
-  const LineLayout Ly(2 * hz, hz, plane, 1, hz, g.fd_2hz, g.fd_hz);
-  cplx<T> *out = smem_fft<T, false, true>(oth, res, Ly, g.py, twy);
-  for (int e = threadIdx.x; e < 2 * plane; e += blockDim.x) {
-    const int c = udiv(e, g.fd_plane), rem = e - c * plane;
-    spec[(2 * p + c) * g.S + (long long)x * plane + rem] = out[e];
-  }
-  if constexpr (PRO >= PRO_TANGENT_TABLE) {
-    __shared__ double red[32];
-    if (u.on) finish_pending_update(a, xx, p * gridDim.x + x, gridDim.x * gridDim.y, red);
+    __syncthreads();
+    const LineLayout Lz(ny, ny, 0, nz, 1, g.fd_ny, g.fd_ny);
+    cplx<T> *res = smem_fft<T, false, false, true>(bufA, bufB, Lz, g.pz, twz);
+    cplx<T> *oth = (res == bufA) ? bufB : bufA;
+    // split the paired transform into the half spectra of components 2p and 2p+1,
+    // laid out [c][y][k] for the y transform
+    for (int e = threadIdx.x; e < plane; e += blockDim.x) {
+      const int y = udiv(e, g.fd_hs), kk = e - y * hs;
+      const cplx<T> Z = res[sidx<true>(y * nz + kk)];
+      const cplx<T> Zm = res[sidx<true>(y * nz + (kk == 0 ? 0 : nz - kk))];
+      oth[e] = mk<T>((T)0.5 * (Z.x + Zm.x), (T)0.5 * (Z.y - Zm.y));
+      oth[plane + e] = mk<T>((T)0.5 * (Z.y + Zm.y), (T)0.5 * (Zm.x - Z.x));
+    }
+    __syncthreads();
+    const LineLayout Ly(2 * hs, hs, plane, 1, hs, g.fd_2hs, g.fd_hs);
+    cplx<T> *out = smem_fft<T, false, true>(oth, res, Ly, g.py, twy);
+    cplx<T> *spec = reinterpret_cast<cplx<T> *>(S.spec);
+    for (int e = threadIdx.x; e < 2 * plane; e += blockDim.x) {
+      const int c = udiv(e, g.fd_plane), rem = e - c * plane;
+      spec[(2 * p + c) * g.S + (long long)x * plane + rem] = out[e];
+    }
+    if constexpr (PRO_IS_KRYLOV(PRO)) {
+      if (u.on) finish_pending_update(S, xx, local, per, red);
+    }
+    __syncthreads();
   }
 }
 
 template <typename T, typename TF, int EPI, int PT>
 __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
-    yzinv_kernel(Grid<T> g, EpiArgs<TF> a, const cplx<T> *__restrict__ spec) {
-  if (EPI == EPI_MINRES && a.st->done) return;
+    yzinv_kernel(Grid<T> g, const SlotDev<TF> *__restrict__ tab, SlotList list, ExtIO<TF> io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[32];
-  const int ny = g.ny, nz = g.nz, hz = g.hz;
-  const int x = blockIdx.x, p = blockIdx.y;
+  __shared__ __align__(16) unsigned char sdesc[sizeof(SlotDev<TF>)];
+  const int ny = g.ny, nz = g.nz, hz = g.hz, hs = g.hs;
+  const long long V = g.V;
   const int cap = padded_len(ny * (nz + 2));
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *bufB = bufA + cap;
@@ -761,104 +878,92 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
   cplx<T> *twz = twy + ny;
   load_table<T>(twy, g.twy, ny);
   load_table<T>(twz, g.twz, nz);
-  const int plane = ny * hz;
-  for (int e = threadIdx.x; e < 2 * plane; e += blockDim.x) {
-    const int c = udiv(e, g.fd_plane), rem = e - c * plane;
-    bufA[e] = spec[(2 * p + c) * g.S + (long long)x * plane + rem];
-  }
-  __syncthreads();
-  const LineLayout Ly(2 * hz, hz, plane, 1, hz, g.fd_2hz, g.fd_hz);
-  cplx<T> *res = smem_fft<T, true, true>(bufA, bufB, Ly, g.py, twy);
-  cplx<T> *oth = (res == bufA) ? bufB : bufA;
-  // full z lines of Z = A + iB from the stored halves (Hermitian in z)
-  for (int e = threadIdx.x; e < ny * nz; e += blockDim.x) {
-    const int y = udiv(e, g.fd_nz), k = e - y * nz;
-    const bool low = (k < hz);
-    const int ks = low ? k : nz - k;
-    const cplx<T> A = res[y * hz + ks];
-    const cplx<T> B = res[plane + y * hz + ks];
-    oth[sidx<true>(e)] = low ? mk<T>(A.x - B.y, A.y + B.x) : mk<T>(A.x + B.y, B.x - A.y);
-  }
-  __syncthreads();
-  const LineLayout Lz(ny, ny, 0, nz, 1, g.fd_ny, g.fd_ny);
-  cplx<T> *fin = smem_fft<T, true, false, true>(oth, res, Lz, g.pz, twz);
-  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-  T c1 = 0;
-  if (EPI == EPI_MINRES) c1 = (T)a.st->c_r1;
-  const long long vbase = (long long)x * ny * nz;
-  const long long o0 = (2 * p) * g.V, o1 = (2 * p + 1) * g.V;
-  if (EPI == EPI_MINRES) {
-    // batches of EPI_BATCH elements per thread: all r1 / r2 loads before the y' stores
-    constexpr int B = EPI_BATCH;
-    const int nel = ny * nz;
-    for (int e0 = threadIdx.x; e0 < nel; e0 += B * blockDim.x) {
-      T l0[B], l1[B], m0[B], m1[B];
-#pragma unroll
-      for (int b = 0; b < B; ++b) {
-        const int e = e0 + b * blockDim.x;
-        if (e < nel) {
-          const long long v = vbase + e;
-          l0[b] = (T)a.r1[o0 + v];
-          l1[b] = (T)a.r1[o1 + v];
-          m0[b] = (T)a.r2[o0 + v];
-          m1[b] = (T)a.r2[o1 + v];
-        }
-      }
-#pragma unroll
-      for (int b = 0; b < B; ++b) {
-        const int e = e0 + b * blockDim.x;
-        if (e < nel) {
-          const long long v = vbase + e;
-          const cplx<T> Z = fin[sidx<true>(e)];
-          const T y0 = Z.x - c1 * l0[b];
-          const T y1 = Z.y - c1 * l1[b];
-          a.out[o0 + v] = (TF)y0;
-          a.out[o1 + v] = (TF)y1;
-          acc0 += (double)m0[b] * (double)y0 + (double)m1[b] * (double)y1;
-          acc1 += (double)y0 * (double)y0 + (double)y1 * (double)y1;
-          acc2 += (double)m0[b] * (double)m0[b] + (double)m1[b] * (double)m1[b];
-        }
-      }
+  const int per = items_plane(g);
+  const int n_items = list_items(list, per);
+  const int plane = ny * hs;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int k = udiv(item, g.fd_it_plane);
+    const int local = item - k * per;
+    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc);
+    if (EPI == EPI_MINRES && block_read_flag(&S.st->done)) continue;
+    const int x = udiv(local, g.fd_3);
+    const int p = local - 3 * x;
+    const cplx<T> *spec = reinterpret_cast<const cplx<T> *>(S.spec);
+    __syncthreads();
+    for (int e = threadIdx.x; e < 2 * plane; e += blockDim.x) {
+      const int c = udiv(e, g.fd_plane), rem = e - c * plane;
+      bufA[e] = spec[(2 * p + c) * g.S + (long long)x * plane + rem];
     }
-  } else {
+    __syncthreads();
+    const LineLayout Ly(2 * hs, hs, plane, 1, hs, g.fd_2hs, g.fd_hs);
+    cplx<T> *res = smem_fft<T, true, true>(bufA, bufB, Ly, g.py, twy);
+    cplx<T> *oth = (res == bufA) ? bufB : bufA;
+    // full z lines of Z = A + iB from the stored halves (Hermitian in z)
     for (int e = threadIdx.x; e < ny * nz; e += blockDim.x) {
-      const long long v = vbase + e;
-      const cplx<T> Z = fin[sidx<true>(e)];
-      a.out[o0 + v] = (TF)Z.x;
-      a.out[o1 + v] = (TF)Z.y;
-      if (EPI == EPI_RESIDUAL) acc0 = fmax(acc0, fmax(fabs((double)Z.x), fabs((double)Z.y)));
+      const int y = udiv(e, g.fd_nz), kk = e - y * nz;
+      const bool low = (kk < hz);
+      const int ks = low ? kk : nz - kk;
+      const bool nyq = 2 * ks == nz;  // the unstored Nyquist column is zero
+      const cplx<T> A = nyq ? mk<T>((T)0, (T)0) : res[y * hs + ks];
+      const cplx<T> B = nyq ? mk<T>((T)0, (T)0) : res[plane + y * hs + ks];
+      oth[sidx<true>(e)] = low ? mk<T>(A.x - B.y, A.y + B.x) : mk<T>(A.x + B.y, B.x - A.y);
     }
-  }
-  if (EPI == EPI_STORE) return;
-  const int blk = blockIdx.y * gridDim.x + blockIdx.x;
-  const int nblk = gridDim.x * gridDim.y;
-  if (EPI == EPI_RESIDUAL) {
-    const double part = block_max(acc0, red);
-    if (threadIdx.x == 0) a.partials[blk] = part;
-  } else {
-    const double q0 = block_sum(acc0, red);
-    const double q1 = block_sum(acc1, red);
-    const double q2 = block_sum(acc2, red);
-    if (threadIdx.x == 0) {
-      a.partials[3 * blk] = q0;
-      a.partials[3 * blk + 1] = q1;
-      a.partials[3 * blk + 2] = q2;
+    __syncthreads();
+    const LineLayout Lz(ny, ny, 0, nz, 1, g.fd_ny, g.fd_ny);
+    cplx<T> *fin = smem_fft<T, true, false, true>(oth, res, Lz, g.pz, twz);
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+    const long long vbase = (long long)x * ny * nz;
+    const int nel = ny * nz;
+    KRoles<TF> kr{};
+    T c1 = 0;
+    if constexpr (EPI == EPI_MINRES) {
+      kr = kroles<TF>(S, S.st->itn);
+      c1 = (T)S.st->c_r1;
+    } else if constexpr (EPI == EPI_REPROJECT) {
+      kr = kroles<TF>(S, 0);
     }
-  }
-  if (!last_block_arrives(a.ticket)) return;
-  if (EPI == EPI_RESIDUAL) {
-    const double m = ordered_max(a.partials, nblk, 1, red);
-    if (threadIdx.x == 0) {
-      *a.result = m;
-      *a.ticket = 0;
+    if constexpr (EPI == EPI_MINRES) {
+      // batches of EPI_BATCH elements per thread: all r1 / r2 loads before the y' stores
+      constexpr int B = EPI_BATCH;
+      const long long o0 = (2 * p) * V, o1 = (2 * p + 1) * V;
+      for (int e0 = threadIdx.x; e0 < nel; e0 += B * blockDim.x) {
+        T l0[B], l1[B], m0[B], m1[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+          const int e = e0 + b * blockDim.x;
+          if (e < nel) {
+            const long long v = vbase + e;
+            l0[b] = (T)kr.P[o0 + v];
+            l1[b] = (T)kr.P[o1 + v];
+            m0[b] = (T)kr.Q[o0 + v];
+            m1[b] = (T)kr.Q[o1 + v];
+          }
+        }
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+          const int e = e0 + b * blockDim.x;
+          if (e < nel) {
+            const long long v = vbase + e;
+            const cplx<T> Z = fin[sidx<true>(e)];
+            const T y0 = Z.x - c1 * l0[b];
+            const T y1 = Z.y - c1 * l1[b];
+            kr.Y[o0 + v] = (TF)y0;
+            kr.Y[o1 + v] = (TF)y1;
+            acc0 += (double)m0[b] * (double)y0 + (double)m1[b] * (double)y1;
+            acc1 += (double)y0 * (double)y0 + (double)y1 * (double)y1;
+            acc2 += (double)m0[b] * (double)m0[b] + (double)m1[b] * (double)m1[b];
+          }
+        }
+      }
+    } else {
+      for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+        const cplx<T> Z = fin[sidx<true>(e)];
+        const T r[2] = {Z.x, Z.y};
+        epilogue_point<T, TF, EPI, 2>(S, io, kr, c1, V, vbase + e, 2 * p, r, nullptr, nullptr,
+                                      acc0, acc1, acc2);
+      }
     }
-  } else {
-    const double d0 = ordered_sum(a.partials, nblk, 3, red);
-    const double d1 = ordered_sum(a.partials + 1, nblk, 3, red);
-    const double d2 = ordered_sum(a.partials + 2, nblk, 3, red);
-    if (threadIdx.x == 0) {
-      minres_after_matvec(a.st, d0, d1, d2);
-      *a.ticket = 0;
-    }
+    finish_inverse<TF, EPI>(S, acc0, acc1, acc2, local, per, red);
+    __syncthreads();
   }
 }

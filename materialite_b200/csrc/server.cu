@@ -1,14 +1,18 @@
-// Serving loop: many RVE homogenisation solves resident on one GPU at once.
+// Serving loop: many RVE homogenisation solves resident on one GPU, batched.
 //
-// Each of `max_slots` worker threads takes the oldest queued request that fits the
-// device-memory budget, builds a solver handle for it (own buffers, own CUDA stream),
-// runs the constant-rate time loop natively (ssfft_solve_constant_rates: Newton with
-// device MINRES replayed from a CUDA graph per handle), copies the final stress out and
-// posts a completion with its queue/start/end times.  Requests that arrive while others
-// run start as soon as a slot and memory are free, and their kernels overlap on the GPU
-// with those of the requests already running.
+// Requests are sorted by class -- grid size, precision, tangent kind (elastic tables or
+// per-voxel crystal-plasticity tangents), slip-system count, and whether the schedule has
+// stress rates -- and each class has a group (group.cuh): up to `max_slots` requests that
+// advance together, every kernel launch covering all of them.  A group's driver thread
+// loads queued requests into free slots (a slot's device memory is allocated on its first
+// use, when it fits both the server's budget and cudaMemGetInfo's free memory), runs the
+// group's rounds graph until some request finishes, returns the finished requests'
+// results, and refills.  Requests that arrive while others run join at the next round
+// boundary of their class; classes run concurrently on their own streams.
 //
-// Only the public C ABI of ssfft.h is used here, plus cudaMemGetInfo for admission.
+// A request's arithmetic does not depend on what else runs: every reduction of a slot is
+// private to it and summed in a fixed order, so a result is bitwise the same alone and in
+// any mix.
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -16,221 +20,235 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
 
 #include "../../include/ssfft.h"
+#include "group_api.h"
 
 int ssfft_internal_fail(int code, const std::string &msg);
 
 namespace {
 
-struct Job {
-  ssfft_request req;  // pointers below replace the caller's borrowed ones
-  std::vector<double> rotations;
-  std::vector<int32_t> orient, phase;
-  double submit_time;
-  size_t bytes;
+struct ClassInfo {
+  bool voxel = false;
+  int nslip = 0;
+  bool rates = false;
+  std::string key;
 };
 
-size_t job_bytes(const ssfft_request &r) {
-  int any_evp = 0, nslip = 0;
+ClassInfo classify(const ssfft_request &r) {
+  ClassInfo c;
   for (int p = 0; p < r.n_phases; ++p)
     if (r.phases[p].kind == 1) {
-      any_evp = 1;
-      nslip = std::max(nslip, (int)r.phases[p].n_slip);
+      c.voxel = true;
+      c.nslip = std::max(c.nslip, (int)r.phases[p].n_slip);
     }
+  for (int k = 0; k < 6; ++k)
+    if (r.schedule.stress_rate[k] * r.config.stress_mask[k] != 0.0) c.rates = true;
+  c.key = std::to_string(r.config.n[0]) + "x" + std::to_string(r.config.n[1]) + "x" +
+          std::to_string(r.config.n[2]) + "/" + std::to_string(r.config.precision) + "/" +
+          std::to_string(c.voxel) + "/" + std::to_string(c.nslip) + "/" + std::to_string(c.rates);
+  return c;
+}
+
+size_t job_bytes(const ssfft_request &r, const ClassInfo &c) {
   size_t b = 0;
-  if (ssfft_estimate_bytes(&r.config, any_evp, nslip, &b) != 0) return 0;
+  if (ssfft_estimate_bytes(&r.config, c.voxel ? 1 : 0, c.nslip, &b) != 0) return 0;
   return b;
 }
 
 }  // namespace
 
-struct PoolEntry {
-  ssfft_handle *h;
-  std::string key;
-  size_t bytes;
-  double last_used;
-};
-
-// Handles are reusable for any request of the same grid, precision and crystal-plasticity
-// shape (ssfft_set_options / ssfft_set_microstructure rebind them).
-std::string pool_key(const ssfft_request &r) {
-  int any_evp = 0, nslip = 0;
-  for (int p = 0; p < r.n_phases; ++p)
-    if (r.phases[p].kind == 1) {
-      any_evp = 1;
-      nslip = std::max(nslip, (int)r.phases[p].n_slip);
-    }
-  return std::to_string(r.config.n[0]) + "x" + std::to_string(r.config.n[1]) + "x" +
-         std::to_string(r.config.n[2]) + "/" + std::to_string(r.config.precision) + "/" +
-         std::to_string(any_evp) + "/" + std::to_string(nslip);
-}
+struct GroupRunner;
 
 struct ssfft_server {
   int device;
+  int max_slots;
   size_t budget;
   std::chrono::steady_clock::time_point t0;
   std::mutex mu;
   std::condition_variable cv;
-  std::deque<Job *> queue;
+  std::map<std::string, std::unique_ptr<GroupRunner>> runners;
   std::vector<ssfft_completion> done;
-  std::vector<std::thread> workers;
-  size_t in_use = 0;  // bytes of every handle alive (running or idle in the pool)
-  int running = 0;
-  std::vector<PoolEntry> idle;
-  long long outstanding = 0;  // submitted, not yet polled
+  size_t in_use = 0;           // bytes of allocated slots
+  long long outstanding = 0;   // submitted, not yet polled
   bool stopping = false;
 
   double now() const {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
+  void post(const ssfft_completion &c) {
+    std::lock_guard<std::mutex> lk(mu);
+    done.push_back(c);
+    cv.notify_all();
+  }
+};
 
-  // Called with mu held.  Grants the oldest job an idle pooled handle of its shape, or
-  // room for a new one.  Idle handles of other shapes are evicted (destroyed outside the
-  // lock, into `evict`) when the budget or the device's free memory is short.
-  bool admit(Job *j, ssfft_handle **pooled, std::vector<ssfft_handle *> &evict) {
-    const std::string key = pool_key(j->req);
-    for (size_t k = 0; k < idle.size(); ++k)
-      if (idle[k].key == key) {
-        *pooled = idle[k].h;
-        j->bytes = idle[k].bytes;
-        idle.erase(idle.begin() + k);
-        return true;
-      }
-    const size_t reserve = (size_t)512 << 20;  // headroom for the runtime and other users
-    for (;;) {
-      size_t free_b = 0, total_b = 0;
-      const bool info = cudaMemGetInfo(&free_b, &total_b) == cudaSuccess;
-      if (info && in_use + j->bytes <= budget && j->bytes + reserve <= free_b) {
-        in_use += j->bytes;
-        return true;
-      }
-      if (idle.empty()) return false;
-      size_t lru = 0;
-      for (size_t k = 1; k < idle.size(); ++k)
-        if (idle[k].last_used < idle[lru].last_used) lru = k;
-      in_use -= idle[lru].bytes;
-      evict.push_back(idle[lru].h);
-      idle.erase(idle.begin() + lru);
-      if (!evict.empty()) return false;  // free them first, then look again
-    }
+struct GroupRunner {
+  ssfft_server *srv;
+  ClassInfo info;
+  ssfft_config proto;
+  Group *g = nullptr;
+  bool init_failed = false;
+  std::string init_message;
+  std::deque<GroupJob *> queue;     // guarded by srv->mu
+  std::vector<GroupJob *> resident; // by slot; touched by the runner thread only
+  std::vector<double> start;        // admission time per slot
+  std::vector<bool> counted;        // slot's bytes counted in srv->in_use
+  std::atomic<long long> launches{0};  // kernels the group has launched (published per run)
+  std::thread th;
+
+  ~GroupRunner() {
+    if (th.joinable()) th.join();
+    for (GroupJob *j : queue) delete j;
+    for (GroupJob *j : resident) delete j;
+    if (g) group_delete(g);
   }
 
-  void run_job(Job *j, int slot, ssfft_handle *h) {
+  ssfft_completion completion(const GroupJob *j, int slot, int status, const char *msg,
+                              double start_time) {
     ssfft_completion c;
     memset(&c, 0, sizeof(c));
     c.tag = j->req.tag;
+    c.status = status;
     c.slot = slot;
     c.submit_time = j->submit_time;
-    c.start_time = now();
+    c.start_time = start_time;
+    c.end_time = srv->now();
     c.device_bytes = j->bytes;
-    ssfft_config cfg = j->req.config;
-    cfg.device = device;
-    int rc = h ? ssfft_set_options(h, &cfg) : ssfft_create(&cfg, &h);
-    for (int p = 0; rc == 0 && p < j->req.n_phases; ++p) {
-      const ssfft_phase &ph = j->req.phases[p];
-      if (ph.kind == 0)
-        rc = ssfft_set_phase_elastic(h, p, ph.stiffness);
-      else
-        rc = ssfft_set_phase_evp(h, p, ph.stiffness, ph.n_slip, ph.schmid,
-                                 ph.reference_slip_rate, ph.rate_exponent, ph.slip_resistance,
-                                 ph.hardening, ph.hardening_props, ph.n_props, ph.latent_ratio);
-    }
-    if (rc == 0)
-      rc = ssfft_set_microstructure(h, j->req.n_orient, j->rotations.data(), j->orient.data(),
-                                    j->phase.empty() ? nullptr : j->phase.data());
-    if (rc == 0) rc = ssfft_solve_constant_rates(h, &j->req.schedule, &c.result);
-    if (rc == 0 && j->req.stress_out) rc = ssfft_get_field(h, SSFFT_FIELD_STRESS, j->req.stress_out, 1);
-    c.status = rc;
-    if (rc != 0) {
-      strncpy(c.message, ssfft_last_error(), sizeof(c.message) - 1);
+    if (msg) {
+      strncpy(c.message, msg, sizeof(c.message) - 1);
       c.message[sizeof(c.message) - 1] = 0;
     }
-    c.end_time = now();
-    const std::string key = pool_key(j->req);
-    const size_t bytes = j->bytes;
-    if (rc != 0 && h) {  // a handle in an unknown state is not reused
-      ssfft_destroy(h);
-      h = nullptr;
+    return c;
+  }
+
+  // Take queued jobs into free slots (mu held).  A slot whose device memory is not yet
+  // allocated is used only when the job fits the budget and the device's free memory.
+  void admit(std::vector<int> &loaded) {
+    const size_t reserve = (size_t)512 << 20;  // headroom for the runtime and other users
+    for (int s = 0; s < srv->max_slots && !queue.empty(); ++s) {
+      if (resident[s]) continue;
+      GroupJob *j = queue.front();
+      if (!counted[s]) {
+        size_t free_b = 0, total_b = 0;
+        const bool info_ok = cudaMemGetInfo(&free_b, &total_b) == cudaSuccess;
+        if (!info_ok || srv->in_use + j->bytes > srv->budget || j->bytes + reserve > free_b)
+          continue;  // try a slot that is already allocated
+        srv->in_use += j->bytes;
+        counted[s] = true;
+      }
+      queue.pop_front();
+      resident[s] = j;
+      start[s] = srv->now();
+      loaded.push_back(s);
     }
-    std::lock_guard<std::mutex> lk(mu);
-    if (h)
-      idle.push_back(PoolEntry{h, key, bytes, c.end_time});
-    else
-      in_use -= bytes;
-    --running;
-    done.push_back(c);
-    delete j;
-    cv.notify_all();
   }
 
-  void fail_job(Job *head, int slot, int code) {  // mu held
-    ssfft_completion c;
-    memset(&c, 0, sizeof(c));
-    c.tag = head->req.tag;
-    c.status = code;
-    c.slot = slot;
-    c.submit_time = head->submit_time;
-    c.start_time = c.end_time = now();
-    c.device_bytes = head->bytes;
-    strncpy(c.message, "request does not fit the device-memory budget", sizeof(c.message) - 1);
-    done.push_back(c);
-    delete head;
+  // Queued jobs that can never be admitted: larger than the whole budget, or, at shutdown,
+  // with no slot allocated and nothing running (mu held).
+  void reject_unfit() {
+    while (!queue.empty()) {
+      GroupJob *j = queue.front();
+      bool any_alloc = false, any_res = false;
+      for (int s = 0; s < srv->max_slots; ++s) {
+        any_alloc = any_alloc || counted[s];
+        any_res = any_res || resident[s];
+      }
+      const bool never = j->bytes > srv->budget || (!any_alloc && !any_res && srv->stopping);
+      if (!never) return;
+      queue.pop_front();
+      srv->done.push_back(completion(j, -1, SSFFT_E_NOMEM,
+                                     "request does not fit the device-memory budget", srv->now()));
+      delete j;
+    }
   }
 
-  void worker(int slot) {
-    cudaSetDevice(device);
+  void run() {
+    cudaSetDevice(srv->device);
+    g = group_new();
+    if (group_init(g, proto, srv->max_slots, info.voxel, info.rates, srv->device) != 0) {
+      init_failed = true;
+      init_message = ssfft_last_error();
+    }
+    resident.assign(srv->max_slots, nullptr);
+    start.assign(srv->max_slots, 0.0);
+    counted.assign(srv->max_slots, false);
     for (;;) {
-      Job *j = nullptr;
-      ssfft_handle *pooled = nullptr;
-      std::vector<ssfft_handle *> evict;
+      std::vector<int> loaded;
       {
-        std::unique_lock<std::mutex> lk(mu);
+        std::unique_lock<std::mutex> lk(srv->mu);
         for (;;) {
-          if (!queue.empty()) {
-            Job *head = queue.front();
-            if (head->bytes > budget) {  // can never fit: fail it now
+          if (init_failed) {
+            while (!queue.empty()) {
+              GroupJob *j = queue.front();
               queue.pop_front();
-              fail_job(head, slot, SSFFT_E_NOMEM);
-              continue;
+              srv->done.push_back(completion(j, -1, SSFFT_E_CUDA, init_message.c_str(), srv->now()));
+              delete j;
             }
-            if (admit(head, &pooled, evict)) {
-              j = head;
-              queue.pop_front();
-              ++running;
-              break;
-            }
-            if (!evict.empty()) break;  // free evicted handles outside the lock, retry
-            if (running == 0 && stopping) {  // nothing will free memory
-              queue.pop_front();
-              fail_job(head, slot, SSFFT_E_NOMEM);
-              continue;
-            }
-          } else if (stopping) {
-            break;
+          } else {
+            reject_unfit();
+            admit(loaded);
           }
-          // wait for a submission or a completion (bounded, so the free-memory check of
-          // cudaMemGetInfo is retried when other processes release memory)
-          cv.wait_for(lk, std::chrono::milliseconds(50));
+          bool any = false;
+          for (GroupJob *j : resident) any = any || j;
+          if (any) break;
+          if (srv->stopping && queue.empty()) {
+            srv->cv.notify_all();
+            return;
+          }
+          // wait for a submission (bounded, so that free memory is looked at again)
+          srv->cv.wait_for(lk, std::chrono::milliseconds(20));
         }
       }
-      for (ssfft_handle *e : evict) ssfft_destroy(e);
-      if (j)
-        run_job(j, slot, pooled);
-      else if (evict.empty()) {
-        std::lock_guard<std::mutex> lk(mu);
-        if (stopping && queue.empty()) return;
+      for (int s : loaded) {
+        if (group_load(g, s, *resident[s]) != 0) {
+          srv->post(completion(resident[s], s, SSFFT_E_CUDA, ssfft_last_error(), start[s]));
+          delete resident[s];
+          resident[s] = nullptr;
+          group_release_slot(g, s);
+        }
+      }
+      bool any = false;
+      for (GroupJob *j : resident) any = any || j;
+      if (!any) continue;
+      const int rc = group_run(g);
+      launches.store(group_launches(g));
+      const std::string msg = rc ? ssfft_last_error() : "";
+      for (int s = 0; s < srv->max_slots; ++s) {
+        GroupJob *j = resident[s];
+        if (!j) continue;
+        const int st = group_slot_state(g, s);
+        if (rc == 0 && st != GS_DONE && st != GS_FAILED) continue;
+        ssfft_completion c = completion(j, s, 0, nullptr, start[s]);
+        group_slot_result(g, s, &c.result);
+        if (rc) {
+          c.status = rc;
+          strncpy(c.message, msg.c_str(), sizeof(c.message) - 1);
+        } else if (st == GS_FAILED) {
+          c.status = c.result.status ? c.result.status : SSFFT_E_INVALID;
+          const char *m = c.status == SSFFT_E_NAN ? "non-finite value in the solve"
+                                                  : "min time increment reached or singular mean tangent";
+          strncpy(c.message, m, sizeof(c.message) - 1);
+        } else if (j->req.stress_out) {
+          if (group_read_stress(g, s, j->req.stress_out) != 0) {
+            c.status = SSFFT_E_CUDA;
+            strncpy(c.message, ssfft_last_error(), sizeof(c.message) - 1);
+          }
+        }
+        c.result.device_seconds = srv->now() - start[s];
+        c.end_time = srv->now();
+        group_release_slot(g, s);
+        delete j;
+        resident[s] = nullptr;
+        srv->post(c);
       }
     }
-  }
-
-  void drain_pool() {
-    for (PoolEntry &e : idle) ssfft_destroy(e.h);
-    idle.clear();
   }
 };
 
@@ -239,17 +257,6 @@ extern "C" int ssfft_server_create(int device, int max_slots, size_t hbm_budget_
   if (!out || max_slots < 1 || max_slots > 256)
     return ssfft_internal_fail(SSFFT_E_INVALID, "max_slots must be 1..256");
   *out = nullptr;
-  // Many slot threads each wait on their own stream; spinning waits compete for the CPU
-  // cores the other slots need to launch work.  SSFFT_SCHEDULE = spin | yield | blocking
-  // selects the waiting mode of the process's CUDA context (before it is created).
-  if (const char *sch = getenv("SSFFT_SCHEDULE")) {
-    unsigned flags = cudaDeviceScheduleAuto;
-    if (!strcmp(sch, "spin")) flags = cudaDeviceScheduleSpin;
-    if (!strcmp(sch, "yield")) flags = cudaDeviceScheduleYield;
-    if (!strcmp(sch, "blocking")) flags = cudaDeviceScheduleBlockingSync;
-    cudaSetDevice(device);
-    if (cudaSetDeviceFlags(flags) != cudaSuccess) cudaGetLastError();
-  }
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return ssfft_internal_fail(SSFFT_E_CUDA, cudaGetErrorString(e));
   size_t free_b = 0, total_b = 0;
@@ -257,9 +264,9 @@ extern "C" int ssfft_server_create(int device, int max_slots, size_t hbm_budget_
   if (e != cudaSuccess) return ssfft_internal_fail(SSFFT_E_CUDA, cudaGetErrorString(e));
   ssfft_server *s = new ssfft_server();
   s->device = device;
+  s->max_slots = max_slots;
   s->budget = hbm_budget_bytes ? hbm_budget_bytes : (size_t)(0.9 * (double)free_b);
   s->t0 = std::chrono::steady_clock::now();
-  for (int k = 0; k < max_slots; ++k) s->workers.emplace_back(&ssfft_server::worker, s, k);
   *out = s;
   return 0;
 }
@@ -270,7 +277,11 @@ extern "C" int ssfft_server_submit(ssfft_server *s, const ssfft_request *req) {
   if (V <= 0 || req->n_orient < 1 || !req->rotations || !req->orient_of_point ||
       req->n_phases < 1 || req->n_phases > SSFFT_MAX_PHASES)
     return ssfft_internal_fail(SSFFT_E_INVALID, "incomplete request");
-  Job *j = new Job();
+  for (int p = 0; p < req->n_phases; ++p)
+    if (req->phases[p].kind != 0 && req->phases[p].kind != 1)
+      return ssfft_internal_fail(SSFFT_E_INVALID, "request phases must be elastic or crystal EVP");
+  const ClassInfo ci = classify(*req);
+  GroupJob *j = new GroupJob();
   j->req = *req;
   j->rotations.assign(req->rotations, req->rotations + 9 * (size_t)req->n_orient);
   j->orient.assign(req->orient_of_point, req->orient_of_point + V);
@@ -278,7 +289,7 @@ extern "C" int ssfft_server_submit(ssfft_server *s, const ssfft_request *req) {
   j->req.rotations = nullptr;
   j->req.orient_of_point = nullptr;
   j->req.phase_of_point = nullptr;
-  j->bytes = job_bytes(j->req);
+  j->bytes = job_bytes(j->req, ci);
   if (j->bytes == 0) {
     delete j;
     return ssfft_internal_fail(SSFFT_E_INVALID, "request configuration rejected");
@@ -288,8 +299,19 @@ extern "C" int ssfft_server_submit(ssfft_server *s, const ssfft_request *req) {
     delete j;
     return ssfft_internal_fail(SSFFT_E_INVALID, "server is shutting down");
   }
+  auto it = s->runners.find(ci.key);
+  if (it == s->runners.end()) {
+    auto r = std::make_unique<GroupRunner>();
+    r->srv = s;
+    r->info = ci;
+    r->proto = j->req.config;
+    r->proto.device = s->device;
+    GroupRunner *rp = r.get();
+    it = s->runners.emplace(ci.key, std::move(r)).first;
+    rp->th = std::thread(&GroupRunner::run, rp);
+  }
   j->submit_time = s->now();
-  s->queue.push_back(j);
+  it->second->queue.push_back(j);
   ++s->outstanding;
   s->cv.notify_all();
   return 0;
@@ -316,6 +338,15 @@ extern "C" int ssfft_server_pending(ssfft_server *s) {
 
 extern "C" double ssfft_server_clock(ssfft_server *s) { return s ? s->now() : 0.0; }
 
+extern "C" int ssfft_server_launches(ssfft_server *s, int64_t *kernel_launches) {
+  if (!s || !kernel_launches) return ssfft_internal_fail(SSFFT_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  long long n = 0;
+  for (auto &kv : s->runners) n += kv.second->launches.load();
+  *kernel_launches = n;
+  return 0;
+}
+
 extern "C" int ssfft_server_destroy(ssfft_server *s) {
   if (!s) return 0;
   {
@@ -323,9 +354,9 @@ extern "C" int ssfft_server_destroy(ssfft_server *s) {
     s->stopping = true;
     s->cv.notify_all();
   }
-  for (auto &t : s->workers) t.join();
-  for (Job *j : s->queue) delete j;
-  s->drain_pool();
+  for (auto &kv : s->runners)
+    if (kv.second->th.joinable()) kv.second->th.join();
+  s->runners.clear();
   delete s;
   return 0;
 }

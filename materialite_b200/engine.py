@@ -147,6 +147,38 @@ class SolverHandle:
     def reset(self):
         nat.check(self.lib.ssfft_reset(self.h))
 
+    def set_options(self, stress_mask=None, global_tolerance=None,
+                    strain_correction_tolerance=None, linear_solver_tolerance=None):
+        """Change the stress mask and tolerances of the handle (same grid and precision)."""
+        cfg = self.cfg
+        if stress_mask is not None:
+            for c in range(6):
+                cfg.stress_mask[c] = float(stress_mask[c])
+        if global_tolerance is not None:
+            cfg.global_tolerance = float(global_tolerance)
+        if strain_correction_tolerance is not None:
+            cfg.strain_correction_tolerance = float(strain_correction_tolerance)
+        if linear_solver_tolerance is not None:
+            cfg.linear_solver_tolerance = float(linear_solver_tolerance)
+        nat.check(self.lib.ssfft_set_options(self.h, ctypes.byref(cfg)))
+
+    def solve_constant_rates(self, strain_rate, stress_rate, end_time, initial_time_increment,
+                             start_time=0.0, max_time_increment=0.0, min_time_increment=0.0):
+        """The whole time loop natively for LoadSchedule.from_constant_rates with the handle's
+        stress mask (ssfft_solve_constant_rates); returns the SsfftSolveOut record."""
+        sc = nat.SsfftRateSchedule()
+        for c in range(6):
+            sc.strain_rate[c] = float(strain_rate[c])
+            sc.stress_rate[c] = float(stress_rate[c])
+        sc.start_time = float(start_time)
+        sc.end_time = float(end_time)
+        sc.initial_time_increment = float(initial_time_increment)
+        sc.max_time_increment = float(max_time_increment)
+        sc.min_time_increment = float(min_time_increment)
+        out = nat.SsfftSolveOut()
+        nat.check(self.lib.ssfft_solve_constant_rates(self.h, ctypes.byref(sc), ctypes.byref(out)))
+        return out
+
     def step(self, dE, dS, Sbar, dt, summed_vm, step_id, reset):
         si = nat.SsfftStepIn()
         for c in range(6):

@@ -1,9 +1,10 @@
 """Serving many RVE homogenisation solves on one GPU (libssfft's ssfft_server_*).
 
 ``RVEServer`` wraps the C server: requests (grid, phases, microstructure, constant-rate
-load schedule) are copied at submission, admitted when a slot and device memory are free,
-solved with their own handle and stream, and returned as completions carrying
-queue/start/end times.  ``request_stream`` generates the seeded request mix of the serving
+load schedule) are copied at submission, join the batched group of their class (grid,
+precision, tangent kind) when a slot and device memory are free, advance together with the
+other requests of the group -- every kernel launch covers all of them -- and come back as
+completions carrying queue/start/end times.  ``request_stream`` generates the seeded request mix of the serving
 benchmark.
 """
 
@@ -61,8 +62,9 @@ def _bind(lib):
     lib.ssfft_server_clock.argtypes = [P]
     lib.ssfft_server_clock.restype = ctypes.c_double
     lib.ssfft_server_destroy.argtypes = [P]
+    lib.ssfft_server_launches.argtypes = [P, ctypes.POINTER(ctypes.c_int64)]
     for n in ("ssfft_server_create", "ssfft_server_submit", "ssfft_server_poll",
-              "ssfft_server_pending", "ssfft_server_destroy"):
+              "ssfft_server_pending", "ssfft_server_destroy", "ssfft_server_launches"):
         getattr(lib, n).restype = ctypes.c_int
     lib._server_bound = True
     return lib
@@ -181,6 +183,12 @@ class RVEServer:
     def pending(self):
         return self.lib.ssfft_server_pending(self.h)
 
+    def kernel_launches(self):
+        """Kernels the server's groups have launched so far."""
+        n = ctypes.c_int64()
+        nat.check(self.lib.ssfft_server_launches(self.h, ctypes.byref(n)))
+        return n.value
+
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:
             self.lib.ssfft_server_destroy(self.h)
@@ -220,18 +228,33 @@ def evp_phase(latent=1.0):
                      {"tau_1": 0.2, "theta_0": 1.0, "theta_1": 0.0}, latent)
 
 
+def request_draws(rng, sizes=(32, 48, 64, 96), grains=(20, 400), steps=(10, 50)):
+    """The scalar draws of one request of the serving mix, in order: grid N ~ U{sizes},
+    G ~ U[20, 400] grains, crystal plasticity with probability 1/2, biaxial with probability
+    1/2, 10-50 load steps.  The microstructure is drawn after these from the same rng."""
+    n = int(rng.choice(sizes))
+    G = int(rng.integers(grains[0], grains[1] + 1))
+    is_evp = bool(rng.random() < 0.5)
+    biaxial = bool(rng.random() < 0.5)
+    nsteps = int(rng.integers(steps[0], steps[1] + 1))
+    return n, G, is_evp, biaxial, nsteps
+
+
+def request_kind(tag, seed=1000, **kw):
+    """Class of request `tag` of the seeded stream ("evp64", "elastic32", ...) and its step
+    count, without building its microstructure."""
+    n, G, is_evp, biaxial, nsteps = request_draws(np.random.default_rng(seed + tag), **kw)
+    return ("evp" if is_evp else "elastic") + f"{n}", nsteps
+
+
 def make_request(tag, rng, sizes=(32, 48, 64, 96), grains=(20, 400), steps=(10, 50)):
     """One request of the serving mix: grid N ~ U{sizes}, G ~ U[20, 400] periodic Voronoi
     grains with uniform SO(3) orientations, elastic or FCC EVP with probability 1/2,
     uniaxial or biaxial constant strain rate 1e-3, 10-50 steps (dt 1 for elastic, 0.2
     for EVP)."""
-    n = int(rng.choice(sizes))
-    G = int(rng.integers(grains[0], grains[1] + 1))
+    n, G, is_evp, biaxial, nsteps = request_draws(rng, sizes, grains, steps)
     ids = periodic_voronoi((n, n, n), G, rng)
     rot = quaternion_random_rotations(G, rng)
-    is_evp = bool(rng.random() < 0.5)
-    biaxial = bool(rng.random() < 0.5)
-    nsteps = int(rng.integers(steps[0], steps[1] + 1))
     rate = np.zeros(6)
     mask = np.ones(6)
     rate[0] = 1e-3
@@ -245,18 +268,35 @@ def make_request(tag, rng, sizes=(32, 48, 64, 96), grains=(20, 400), steps=(10, 
                       steps=nsteps, kind=("evp" if is_evp else "elastic") + f"{n}")
 
 
-def request_stream(count, rate, seed=1000, **kw):
+def _make_tagged(args):
+    tag, seed, kw = args
+    return make_request(tag, np.random.default_rng(seed + tag), **kw)
+
+
+def arrival_times(count, rate, seed=1000):
+    """Poisson arrival times of a stream of `count` requests at `rate` per second (rate <=
+    0: all at t = 0), drawn from np.random.default_rng(seed - 1)."""
+    if rate <= 0:
+        return np.zeros(count)
+    return np.cumsum(np.random.default_rng(seed - 1).exponential(1.0 / rate, size=count))
+
+
+def request_stream(count, rate, seed=1000, workers=1, tags=None, **kw):
     """``count`` requests with Poisson arrival times at ``rate`` per second (rate <= 0:
-    all at t = 0).  Request i draws from np.random.default_rng(seed + i)."""
-    reqs = []
-    arr_rng = np.random.default_rng(seed - 1)
-    t = 0.0
-    for i in range(count):
-        r = make_request(i, np.random.default_rng(seed + i), **kw)
-        if rate > 0:
-            t += arr_rng.exponential(1.0 / rate)
-        r.arrival = t if rate > 0 else 0.0
-        reqs.append(r)
+    all at t = 0).  Request i draws from np.random.default_rng(seed + i).  ``workers`` > 1
+    builds the microstructures in that many spawned processes; ``tags`` selects requests of
+    the stream (they keep their arrival times)."""
+    tags = list(range(count)) if tags is None else list(tags)
+    arrivals = arrival_times(max(tags) + 1 if tags else 0, rate, seed)
+    jobs = [(t, seed, kw) for t in tags]
+    if workers > 1 and len(jobs) > 1:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(workers) as pool:
+            reqs = pool.map(_make_tagged, jobs, chunksize=4)
+    else:
+        reqs = [_make_tagged(j) for j in jobs]
+    for r in reqs:
+        r.arrival = float(arrivals[r.tag]) if rate > 0 else 0.0
     return reqs
 
 
@@ -291,3 +331,33 @@ def latency_stats(completions, requests=None):
     lat = np.array([c.end_time - c.submit_time for c in completions])
     return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_s": float(lat.mean()), "max_s": float(lat.max())}
+
+
+def solve_plain(requests, precision="fp64", device=0, keep_stress=True):
+    """The plain single-request GPU solve: each request alone, one after another, through a
+    solver handle running the native time loop (ssfft_solve_constant_rates); one handle per
+    grid size is reused.  Stores each request's final stress in ``r.stress`` (keep_stress)
+    and returns (per-request seconds, solve records)."""
+    import time
+    from .engine import SolverHandle
+    handles = {}
+    secs, outs = [], []
+    try:
+        for r in requests:
+            t0 = time.perf_counter()
+            h = handles.get(tuple(r.dims))
+            if h is None:
+                h = SolverHandle(r.dims, r.stress_mask, precision, device=device)
+                handles[tuple(r.dims)] = h
+            h.set_options(r.stress_mask, r.global_tolerance, 1e-2, r.linear_solver_tolerance)
+            h.set_phases(r.phases)
+            h.set_microstructure(r.rotations, r.grain, r.phase_of_point)
+            out = h.solve_constant_rates(r.strain_rate, r.stress_rate, r.dt * r.steps, r.dt)
+            if keep_stress:
+                r.stress = h.field("stress")
+            secs.append(time.perf_counter() - t0)
+            outs.append(out)
+    finally:
+        for h in handles.values():
+            h.close()
+    return secs, outs

@@ -82,3 +82,63 @@ def test_admission_by_memory_budget():
     assert all(c.status == 0 for c in comps)
     a, b = sorted(comps, key=lambda c: c.start_time)
     assert b.start_time >= a.end_time
+
+
+def evp_requests(seeds, steps=(3, 5)):
+    rs = []
+    for tag, seed in enumerate(seeds):
+        r = make_request(tag, np.random.default_rng(seed), sizes=(32,), grains=(20, 60),
+                         steps=steps)
+        r.phases = [evp_phase()]
+        r.dt = 0.2
+        r.keep_stress = True
+        rs.append(r)
+    return rs
+
+
+def test_batched_requests_identical_alone_and_in_the_group():
+    """Four crystal-plasticity requests of one class share a group: every kernel launch
+    covers all four, their Newton iterations advance in common rounds, and each result is
+    still bitwise the one it gets alone (every reduction is private to its slot)."""
+    seeds = [31, 32, 33, 34]
+    alone = []
+    for r in evp_requests(seeds):
+        srv = RVEServer(max_slots=1)
+        comps, _ = run_stream(srv, [r])
+        srv.close()
+        assert comps[0].status == 0
+        alone.append(r.stress.copy())
+    mix = evp_requests(seeds)
+    srv = RVEServer(max_slots=4)
+    comps, _ = run_stream(srv, mix)
+    launches = srv.kernel_launches()
+    srv.close()
+    assert all(c.status == 0 for c in comps)
+    for r, a in zip(mix, alone):
+        assert np.array_equal(r.stress, a)
+    starts = sorted(c.start_time for c in comps)
+    ends = sorted(c.end_time for c in comps)
+    assert starts[-1] < ends[0]  # all four were resident at the same time
+    assert launches > 0
+
+
+def test_group_time_loop_matches_python_loop_crystal_plasticity():
+    """The device-side Newton decisions, commits and dt updates of a group reproduce the
+    host-driven time loop (engine.solve through a handle) bitwise for a crystal-plasticity
+    request."""
+    r = evp_requests([41], steps=(4, 4))[0]
+    server = RVEServer(max_slots=2)
+    comps, _ = run_stream(server, [r])
+    server.close()
+    assert comps[0].status == 0
+    h = SolverHandle(r.dims, r.stress_mask, "mixed", global_tolerance=r.global_tolerance,
+                     linear_solver_tolerance=r.linear_solver_tolerance)
+    h.set_phases(r.phases)
+    table, idx = unique_rotations(r.rotations[r.grain])
+    h.set_microstructure(table, idx)
+    er = r.strain_rate * (1 - r.stress_mask)
+    z = np.zeros(6)
+    out, _ = solve(h, lambda t, dt: er * dt, lambda t, dt: z, lambda t, dt: z,
+                   end_time=r.dt * r.steps, initial_time_increment=r.dt)
+    h.close()
+    assert np.array_equal(out["stress"], r.stress)
