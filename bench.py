@@ -1,14 +1,18 @@
 """Benchmark of the SmallStrainFFT solve on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload plain128]
+                    [--workload serve|plain128|...] [--mode bench|kernels|request|accuracy|sweep]
 
-One "step" is one complete RVE solve of the workload (every load increment, Newton
-iterations and device MINRES), with the microstructure already resident in HBM.
-Multi-GPU runs are independent replicas (one RVE solve stream per GPU; the path has no
-exchange step), so ``scaling`` is "weak".
+Default workload: the serving stream of BASELINE config 4 -- 512 RVE requests arriving as
+a Poisson process at 50 req/s, N ~ U{32,48,64,96}, 20-400 periodic Voronoi grains,
+elastic or FCC crystal plasticity, uniaxial or biaxial strain rate, 10-50 load steps --
+served on one warm server.  The K timed steps are K consecutive slices of that stream (by
+arrival), run as one continuous stream; beside the headline the line carries the served
+throughput and latency at 1-20 req/s, the plain single-request FP64 GPU solve of a prefix
+of the stream, and CPU numbers measured on complete solves of the stream's requests.
 
-Prints one JSON line (rank 0).
+Multi-GPU runs are replicas: the stream is partitioned across ranks (no exchange step),
+so ``scaling`` is "strong".  Prints one JSON line (rank 0).
 """
 
 import argparse
@@ -51,8 +55,13 @@ WORKLOADS = {
                         ltol=1e-5, precision="mixed", seed=0, model="twophase"),
     # Serving stream: requests with N ~ U{32,48,64,96}, 20-400 periodic Voronoi grains,
     # elastic or FCC EVP (p = 1/2), uniaxial or biaxial strain rate 1e-3, 10-50 steps,
-    # Poisson arrivals; the first `count` requests of the seeded stream.
-    "serve": dict(count=24, rate=50.0, slots=16, seed=1000),
+    # Poisson arrivals at 50 req/s; the first `count` requests of the seeded stream.
+    # Beside it: the sweep rates (each over the prefix that arrives in `sweep_seconds`),
+    # the plain FP64 single-request solve of the first `plain_count` requests, and the
+    # stream's 32^3 elastic requests among the first `cpu_count` (the CPU-feasible class,
+    # solved in full by the CPU baselines).
+    "serve": dict(count=512, rate=50.0, slots=16, seed=1000, sweep_rates=(1, 2, 5, 10, 20),
+                  sweep_seconds=20.0, plain_count=48, e2e_count=128, cpu_count=512),
 }
 
 def plane_path(n):
@@ -63,12 +72,13 @@ def plane_path(n):
 
 
 # Algorithmic HBM bytes per voxel of each Krylov-iteration kernel with float fields:
-# planar vectors are 24 B/voxel (6 x 4 B); the half spectrum is 6 x (n/2+1)/n x 8 B.  The
+# planar vectors are 24 B/voxel (6 x 4 B); the stored half spectrum is 6 x hs/n x 8 B with
+# hs = n/2 columns on even grids (the zeroed Nyquist column is not stored), (n+1)/2 on odd.  The
 # forward z pass also applies the previous iteration's vector update (reads y', u, w1,
 # w2, x; writes u', w, x).  With the plane-fused passes the y transforms happen in shared
 # memory inside the z kernels and move no bytes of their own.
 def kernel_bytes_per_voxel(n, table_mode=True):
-    spec = 6 * (n // 2 + 1) / n * 8.0
+    spec = 6 * (n // 2 if n % 2 == 0 else n // 2 + 1) / n * 8.0
     kin = 4.0 if table_mode else 84.0
     ypass = 0.0 if plane_path(n) else 2 * spec
     return {
@@ -227,56 +237,44 @@ def cpu_sample(w, max_seconds=40.0):
     return per_solve, t_build, t_first
 
 
-SERVE_SAMPLE_STEPS = 3
+CPU_CLASS = "elastic32"
 
 
-def cpu_serve_sample(seed=1000):
-    """Time the numpy oracle (this process, one core) on the first SERVE_SAMPLE_STEPS
-    load increments of a 32^3 elastic request and a 32^3 EVP request of the serving mix,
-    plus the 32^3 Gamma-hat build.  Returns seconds per increment per kind and the build
-    time."""
+def cpu_subset_tags(w, count=None):
+    """Tags of the stream's 32^3 elastic requests (stream order): the class that a CPU solves
+    in full within seconds (a 96^3 crystal-plasticity request takes hours on one core)."""
+    from materialite_b200.serving import request_kind
+    n = count or w["cpu_count"]
+    return [t for t in range(n) if request_kind(t, w["seed"])[0] == CPU_CLASS]
+
+
+def oracle_solve_request(r):
+    """The numpy oracle (the reference's numpy path restated) on one request of the stream,
+    in full; returns seconds and the final stress (V, 6)."""
     from oracle import ssfft_oracle as O
-    from materialite_b200.serving import cubic, elastic_phase, evp_phase, make_request
-    out = {}
+    from materialite_b200.serving import cubic
     t0 = time.perf_counter()
-    O.projection_operator((32, 32, 32), [0, 1, 1, 1, 1, 1])
-    out["build32"] = time.perf_counter() - t0
-    for kind in ("elastic", "evp"):
-        r = make_request(0, np.random.default_rng(seed), sizes=(32,), grains=(100, 100),
-                         steps=(10, 10))
-        if kind == "evp":
-            p = evp_phase()
-            model = O.EVPOracle(p.stiffness, p.schmid, p.reference_slip_rate, p.rate_exponent,
-                                p.slip_resistance, "voce", p.hardening_props)
-            dt = 0.2
-        else:
-            model = O.ElasticOracle(cubic(250.0, 150.0, 120.0))
-            dt = 1.0
-        load = O.LoadOracle.constant_rates(r.strain_rate, np.zeros(6), r.stress_mask)
-        t0 = time.perf_counter()
-        O.solve(r.dims, r.rotations[r.grain], model, load, end_time=SERVE_SAMPLE_STEPS * dt,
-                initial_time_increment=dt, global_tolerance=r.global_tolerance,
-                linear_solver_tolerance=r.linear_solver_tolerance)
-        out[kind] = (time.perf_counter() - t0 - out["build32"]) / SERVE_SAMPLE_STEPS
-    return out
+    p = r.phases[0]
+    if p.kind == "evp":
+        model = O.EVPOracle(p.stiffness, p.schmid, p.reference_slip_rate, p.rate_exponent,
+                            p.slip_resistance, "voce", p.hardening_props)
+    else:
+        model = O.ElasticOracle(cubic(250.0, 150.0, 120.0))
+    load = O.LoadOracle.constant_rates(r.strain_rate, np.zeros(6), r.stress_mask)
+    out = O.solve(r.dims, r.rotations[r.grain], model, load, end_time=r.steps * r.dt,
+                  initial_time_increment=r.dt, global_tolerance=r.global_tolerance,
+                  linear_solver_tolerance=r.linear_solver_tolerance)
+    return time.perf_counter() - t0, out["stress"]
 
 
-def cpu_serve_seconds(reqs, sample):
-    """Extrapolated oracle seconds per request: (Gamma-hat build + steps x seconds per
-    increment of its kind) x (N/32)^3."""
-    per = []
-    for r in reqs:
-        scale = (r.dims[0] / 32.0) ** 3
-        kind = "evp" if r.kind.startswith("evp") else "elastic"
-        per.append((sample["build32"] + r.steps * sample[kind]) * scale)
-    return float(np.mean(per))
-
-
-SERVE_SAMPLE_TEXT = (f"numpy oracle on the first {SERVE_SAMPLE_STEPS} load increments of a 32^3 "
-                     "elastic and a 32^3 FCC EVP request plus the 32^3 Gamma-hat build, "
-                     "extrapolated to every request of the stream by its step count and "
-                     "(N/32)^3; EVP increments after the onset of slip need more Newton "
-                     "iterations than the sampled ones, so this underestimates the CPU time")
+def _ref_solve_tag(args):
+    """Worker of the CPU pools: build request `tag` of the stream and solve it in full with
+    the oracle (one thread)."""
+    tag, seed = args
+    from materialite_b200.serving import make_request
+    r = make_request(tag, np.random.default_rng(seed + tag))
+    secs, _ = oracle_solve_request(r)
+    return tag, secs
 
 
 SINGLE_THREAD_ENV = {"OMP_NUM_THREADS": "1", "OPENBLAS_NUM_THREADS": "1",
@@ -291,53 +289,99 @@ def single_thread_pool(workers):
     return mp.get_context("spawn").Pool(workers)
 
 
-def reference_arm(args, w):
-    """--impl reference: the oracle restatement of the reference's numpy path on the host
-    cores (the reference is pure Python; the oracle matches it to 1e-15).  Each step runs a
-    bounded sample in every worker process at once; value = workers / extrapolated seconds
-    per solve."""
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
-    import multiprocessing as mp
+def host_workers():
     cores = os.cpu_count() or 1
     try:
         import psutil
-        mem_workers = max(1, int(psutil.virtual_memory().available / (12 * 2**30)))
+        mem_workers = max(1, int(psutil.virtual_memory().available / (2 * 2**30)))
     except Exception:
         mem_workers = 4
-    serve = args.workload == "serve"
-    workers = max(1, min(cores, mem_workers, 16))
+    return max(1, min(cores, mem_workers))
+
+
+def _ref_worker(w):
+    return cpu_sample(w)
+
+
+def reference_arm_single(args, w):
+    """--impl reference for a single-solve workload (plain128, ...): every host core runs the
+    oracle on the workload's Gamma-hat build and first load increment, extrapolated to the
+    workload's increments (a full 128^3 CPU solve takes tens of minutes); the sample says
+    so."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    workers = max(1, min(host_workers(), 8))
     times = []
-    reqs = None
-    if serve:
-        from materialite_b200.serving import request_stream
-        reqs = request_stream(args.count or w["count"], w["rate"], seed=w["seed"])
     with single_thread_pool(workers) as pool:
         for i in range(args.warmup + args.steps):
-            if serve:
-                res = pool.map(_ref_serve_worker, [w["seed"]] * workers)
-                worst = {k: max(r[k] for r in res) for k in res[0]}
-                t = cpu_serve_seconds(reqs, worst)
-            else:
-                res = pool.map(_ref_worker, [w] * workers)
-                t = max(r[0] for r in res)
+            res = pool.map(_ref_worker, [w] * workers)
             if i >= args.warmup:
-                times.append(t)
+                times.append(max(r[0] for r in res))
     per_solve = statistics.mean(times)
     value = workers / per_solve
-    if serve:
-        cfg = {"workload": f"serve: {len(reqs)} requests of the serving stream (see the ours line)"}
-        sample = SERVE_SAMPLE_TEXT
-    else:
-        cfg = {"workload": args.workload, **{k: w[k] for k in ("n", "grains", "steps")}}
-        sample = ("per worker: Gamma-hat build + first load increment, extrapolated to all "
-                  "load increments")
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_solve * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded periodic Voronoi, uniform SO(3))",
-            "impl": "reference", "config": cfg,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded periodic Voronoi, uniform SO(3))", "impl": "reference",
+            "config": {"workload": args.workload, **{k: w[k] for k in ("n", "grains", "steps")}},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers, "kind": "port",
+                             "sample": "per worker: Gamma-hat build + first load increment, "
+                                       "extrapolated to all load increments"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def serve_config(w, count):
+    return {"workload": f"serve: {count} requests of the seeded serving stream (BASELINE config "
+                        f"4), Poisson arrivals at {w['rate']} req/s, N in {{32,48,64,96}}, 20-400 "
+                        "periodic Voronoi grains, elastic or FCC EVP, uniaxial/biaxial strain "
+                        "rate 1e-3, 10-50 load steps; one step = one slice of the stream by "
+                        "arrival, the stream run once continuously",
+            "count": count, "rate_per_s": w["rate"],
+            "sweep_rates_per_s": list(w["sweep_rates"]) + [w["rate"]]}
+
+
+def reference_arm(args, w):
+    """--impl reference: the reference's numpy path (the oracle restatement; the reference is
+    pure Python and the oracle matches it to 1e-15) on every host core.  A CPU solves the
+    stream's 32^3 elastic requests in seconds but its 96^3 crystal-plasticity requests in
+    hours, so the arm measures complete solves of the 32^3 elastic requests of the stream:
+    one worker process per core works through them continuously; a step is one completed
+    request; after W warm-up completions, value = K completions / the time they took."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    tags = cpu_subset_tags(w)
+    workers = host_workers()
+    need = args.warmup + args.steps + workers
+    todo = [(tags[i % len(tags)], w["seed"]) for i in range(need)]
+    done_t = []
+    pool = single_thread_pool(workers)
+    try:
+        t_start = time.perf_counter()
+        for _tag, _secs in pool.imap_unordered(_ref_solve_tag, todo):
+            done_t.append(time.perf_counter())
+            if len(done_t) >= args.warmup + args.steps:
+                break
+    finally:
+        pool.terminate()
+        pool.join()
+    t0 = done_t[args.warmup - 1] if args.warmup > 0 else t_start
+    t1 = done_t[args.warmup + args.steps - 1]
+    value = args.steps / (t1 - t0)
+    sample = (f"numpy oracle, complete solves of the stream's {CPU_CLASS} requests "
+              f"({len(tags)} of the first {w['cpu_count']}, cycled in stream order), "
+              f"{workers} single-threaded worker processes working continuously; one step = "
+              "one completed request, timed after the warm-up completions")
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": (t1 - t0) / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded request stream: periodic Voronoi, "
+                                    "uniform SO(3))",
+            "impl": "reference", "config": serve_config(w, args.count or w["count"]),
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers,
                              "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
@@ -345,138 +389,176 @@ def reference_arm(args, w):
     print(json.dumps(line), flush=True)
 
 
-def _ref_worker(w):
-    return cpu_sample(w)
-
-
-def _ref_serve_worker(seed):
-    return cpu_serve_sample(seed)
-
-
 def serve_mode(args, w):
-    """Serving benchmark on one warm server: W untimed and K timed passes of the seeded
-    request stream (Poisson arrivals, up to `slots` requests resident, mixed precision);
-    then the same stream end to end with every request's stress field read back to the
-    host, the saturated stream (all arrivals at 0), and the plain single-request FP64 GPU
-    solve (one slot, requests one after another) with the stress error of mixed against
-    it.  Under torchrun every rank serves its own stream (replicas)."""
+    """Serving benchmark of BASELINE config 4 on one warm server (mixed precision): the
+    W warm-up steps serve one request of every class of the stream at once; the K timed
+    steps are the whole stream at its Poisson arrivals (one continuous run).  Then: the same
+    stream's prefix end to end with every stress field read back, the sweep of arrival
+    rates, the plain single-request FP64 GPU solve of a prefix against the served solve of
+    the same requests (throughput and stress error), the 32^3 elastic requests the CPU
+    baselines solve, the 128^3 roofline, and the one-core CPU baseline.  Under torchrun the
+    stream is partitioned across the ranks (replicas)."""
     from materialite_b200 import replicas
-    from materialite_b200.serving import RVEServer, latency_stats, request_stream, run_stream
-    world, rank, local = replicas.init("nccl")
+    from materialite_b200.serving import (RVEServer, arrival_times, latency_stats,
+                                          request_stream, run_stream, solve_plain)
     count = args.count or w["count"]
-    reqs = request_stream(count, w["rate"], seed=w["seed"] + 1000 * rank)
+    # every request is built before the first GPU call (spawned pool)
+    reqs_all = request_stream(count, w["rate"], seed=w["seed"], workers=host_workers())
+    world, rank, local = replicas.init("nccl")
+    reqs = replicas.partition(reqs_all, world, rank) if world > 1 else reqs_all
+    per_step = -(-len(reqs) // args.steps)
     voxels = sum(int(np.prod(r.dims)) for r in reqs)
-    h2d = sum(r.grain.nbytes + r.rotations.nbytes for r in reqs)
+    classes = {}
+    for r in reqs:
+        classes.setdefault(r.kind, r)
 
-    def one_pass(srv, keep, saturate=False):
-        arrivals = [r.arrival for r in reqs]
-        for r in reqs:
-            r.keep_stress = keep
-            if saturate:
+    def one_pass(srv, rs, keep, rate=None, saturate=False):
+        saved = [r.arrival for r in rs]
+        if rate is not None:
+            for r, t in zip(rs, arrival_times(len(rs), rate, w["seed"])):
+                r.arrival = float(t)
+        if saturate:
+            for r in rs:
                 r.arrival = 0.0
-        comps, span = run_stream(srv, reqs, timeout=1800)
-        for r, a in zip(reqs, arrivals):
-            r.arrival = a
+        t0 = min(r.arrival for r in rs)
+        for r in rs:
+            r.keep_stress = keep
+            r.arrival -= t0
+        try:
+            comps, span = run_stream(srv, rs, timeout=3600)
+        finally:
+            for r, a in zip(rs, saved):
+                r.arrival = a
         bad = [(c.tag, c.status, c.message.decode(errors="replace")) for c in comps
                if c.status != 0]
         if bad:
             raise RuntimeError(f"requests failed: {bad}")
         return comps, span
 
+    import torch
     srv = RVEServer(device=local, max_slots=w["slots"], precision="mixed")
+    warm = list(classes.values())
     for _ in range(args.warmup):
-        one_pass(srv, False)
+        one_pass(srv, warm, False, saturate=True)
+    torch.cuda.synchronize(local)
     replicas.barrier(world)
     sampler = ClockSampler(local)
     sampler.start()
-    spans, comps_all = [], []
-    for _ in range(args.steps):
-        comps, span = one_pass(srv, False)
-        spans.append(span)
-        comps_all += comps
+    l0 = srv.kernel_launches()
+    comps, span = one_pass(srv, reqs, False)
+    l1 = srv.kernel_launches()
+    torch.cuda.synchronize(local)
     clocks = sampler.stop()
-    launches = sum(int(c.result.kernel_launches) for c in comps_all)
-    t_served = replicas.max_over_ranks(sum(spans), world, local)
-    total = replicas.sum_over_ranks(count * args.steps, world, local)
-    value = total / t_served
-    lat = latency_stats(comps_all)
-    # end to end: the same stream with each request's stress field copied to the host
-    e2e_spans = []
-    for _ in range(max(1, args.e2e_steps)):
-        _, span = one_pass(srv, True)
-        e2e_spans.append(span)
-    stress_mixed = [r.stress.copy() for r in reqs]
-    t_e2e = replicas.max_over_ranks(sum(e2e_spans), world, local)
-    e2e_value = replicas.sum_over_ranks(count * len(e2e_spans), world, local) / t_e2e
-    _, span_sat = one_pass(srv, False, saturate=True)
+    t_max = replicas.max_over_ranks(span, world, local)
+    total = replicas.sum_over_ranks(len(reqs), world, local)
+    value = total / t_max
+    lat = latency_stats(comps)
+    kinds = {}
+    for r, c in zip(reqs, comps):
+        kinds.setdefault(r.kind, []).append(c.end_time - c.submit_time)
+    per_class = {k: {"count": len(v), "p50_s": float(np.percentile(v, 50)),
+                     "p99_s": float(np.percentile(v, 99))} for k, v in sorted(kinds.items())}
+    # end to end: a prefix of the stream with every stress field copied to the host
+    e2e_reqs = reqs[:min(len(reqs), w["e2e_count"])]
+    _, span_e2e = one_pass(srv, e2e_reqs, True)
+    e2e_value = replicas.sum_over_ranks(len(e2e_reqs), world, local) / \
+        replicas.max_over_ranks(span_e2e, world, local)
+    h2d = sum(r.grain.nbytes + r.rotations.nbytes for r in e2e_reqs) / max(1, len(e2e_reqs))
+    d2h = sum(int(np.prod(r.dims)) * 48 for r in e2e_reqs) / max(1, len(e2e_reqs))
+    # arrival-rate sweep: each rate over the prefix that arrives in sweep_seconds
+    sweep = []
+    for rate in w["sweep_rates"]:
+        n = max(8, min(len(reqs), int(w["sweep_seconds"] * rate)))
+        cs, sp = one_pass(srv, reqs[:n], False, rate=rate)
+        sweep.append({"rate_per_s": rate, "count": n, "solves_per_s": n / sp, **latency_stats(cs)})
+    sweep.append({"rate_per_s": w["rate"], "count": len(reqs), "solves_per_s": len(reqs) / span,
+                  **lat})
+    # plain single-request FP64 GPU solve of a prefix, against the served mixed solve of the
+    # same requests (all submitted at once)
+    sub = reqs[:min(len(reqs), w["plain_count"])]
+    _, span_sub = one_pass(srv, sub, True, saturate=True)
+    stress_mixed = [r.stress.copy() for r in sub]
     srv.close()
-    plain_srv = RVEServer(device=local, max_slots=1, precision="fp64")
-    plain, span_plain = one_pass(plain_srv, True, saturate=True)
-    plain_srv.close()
-    stress_fp64 = [r.stress.copy() for r in reqs]
+    secs_plain, _ = solve_plain(sub, "fp64", device=local)
+    stress_fp64 = [r.stress.copy() for r in sub]
     errs = [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(stress_mixed, stress_fp64)]
-    span_sat = replicas.max_over_ranks(span_sat, world, local)
-    span_plain = replicas.max_over_ranks(span_plain, world, local)
-    count_all = replicas.sum_over_ranks(count, world, local)
-    lat_plain = latency_stats(plain)
+    plain_value = len(sub) / sum(secs_plain)
+    served_sub = len(sub) / span_sub
+    # the CPU class (32^3 elastic requests of the stream), on the GPU: served and plain
+    cpu_tags = set(cpu_subset_tags(w, count))
+    cpu_reqs = [r for r in reqs if r.tag in cpu_tags]
+    cpu_gpu = None
+    if cpu_reqs:
+        srv2 = RVEServer(device=local, max_slots=w["slots"], precision="mixed")
+        _, span_c = one_pass(srv2, cpu_reqs, False, saturate=True)
+        srv2.close()
+        secs_c, _ = solve_plain(cpu_reqs, "fp64", device=local, keep_stress=False)
+        cpu_gpu = {"workload": f"the stream's {len(cpu_reqs)} {CPU_CLASS} requests among the "
+                               f"first {count}",
+                   "served_solves_per_s": len(cpu_reqs) / span_c,
+                   "plain_fp64_solves_per_s": len(cpu_reqs) / sum(secs_c)}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": t_served / args.steps * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "ms_per_step": t_max / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded request stream: periodic Voronoi, uniform SO(3))",
-            "config": {"workload": f"serve: one step = one pass of {count} requests of the "
-                                   f"serving stream at {w['rate']} req/s Poisson, N in "
-                                   "{32,48,64,96}, 20-400 grains, elastic or FCC EVP, "
-                                   "uniaxial/biaxial, 10-50 steps; "
-                                   f"{w['slots']} resident slots, float fields with double "
-                                   "residuals/norms/EVP Newton",
-                       "parallelism": f"replicas x{world}", "voxels_per_step": voxels,
-                       "l2": "inputs larger than L2: one pass streams every request's "
-                             "fields through HBM; each request's own solve runs L2-resident "
-                             "as it does in service"},
-            "served": {"solves_per_s": value, **lat, "makespan_s_per_step": t_served / args.steps},
-            "saturation": {"solves_per_s": count_all / span_sat, "makespan_s": span_sat},
-            "plain_fp64_single_request": {"solves_per_s": count_all / span_plain,
-                                          **{k: v for k, v in lat_plain.items()},
-                                          "makespan_s": span_plain},
-            "served_over_plain": value / (count_all / span_plain),
-            "stress_rel_l2_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs))},
+            "config": {**serve_config(w, count),
+                       "requests_per_step": per_step,
+                       "parallelism": f"replicas x{world} (stream partitioned by cost)",
+                       "slots_per_class": w["slots"], "voxels": voxels,
+                       "precision": "float fields and FFTs; double residuals, norms, Krylov "
+                                    "scalars and crystal-plasticity Newton",
+                       "l2": "inputs larger than L2: the stream's fields stream through HBM"},
+            "served": {"solves_per_s": value, **lat, "makespan_s": t_max,
+                       "per_class_latency": per_class},
+            "sweep": sweep,
+            "plain_fp64_single_request": {"workload": f"first {len(sub)} requests of the "
+                                                      "stream, one at a time",
+                                          "solves_per_s": plain_value,
+                                          "served_solves_per_s_same_requests": served_sub},
+            "served_over_plain": served_sub / plain_value,
+            "stress_rel_l2_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs)),
+                                            "requests": len(errs)},
+            "cpu_class_on_gpu": cpu_gpu,
             "clocks": clocks,
-            "gpu_launches": launches,
+            "gpu_launches": int(l1 - l0),
             "e2e": {"value": e2e_value, "unit": "solves/s",
-                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(voxels * 48),
-                    "note": "requests submitted from host numpy arrays (grain ids, "
-                            "rotations), stress fields copied back to host numpy arrays"},
+                    "h2d_bytes_per_step": int(h2d * per_step),
+                    "d2h_bytes_per_step": int(d2h * per_step),
+                    "workload": f"first {len(e2e_reqs)} requests of the stream at "
+                                f"{w['rate']} req/s, submitted from host numpy arrays, every "
+                                "stress field copied back to a host numpy array"},
         }
         if not args.no_roofline:
             line["roofline"] = plain128_roofline(local)
-        if world == 1 and not args.no_cpu_baseline:
-            with single_thread_pool(1) as pool:
-                sample = pool.map(_ref_serve_worker, [w["seed"]])[0]
-            per = cpu_serve_seconds(reqs, sample)
-            line["cpu_baseline"] = {"value": 1.0 / per, "unit": "solves/s", "cores": 1,
-                                    "kind": "port", "sample": SERVE_SAMPLE_TEXT}
+        if world == 1 and not args.no_cpu_baseline and cpu_reqs:
+            secs, _ = oracle_solve_request(cpu_reqs[0])
+            line["cpu_baseline"] = {
+                "value": 1.0 / secs, "unit": "solves/s", "cores": 1, "kind": "port",
+                "sample": f"numpy oracle (the reference's numpy path), one complete solve of "
+                          f"request {cpu_reqs[0].tag} of the stream ({cpu_reqs[0].kind}, "
+                          f"{cpu_reqs[0].steps} load steps) on one core: {secs:.1f} s"}
         print(json.dumps(line), flush=True)
     replicas.destroy(world)
 
 
 def sweep_mode(args, w):
-    """Arrival-rate sweep of the serving stream on one warm server: the same seeded
+    """Arrival-rate sweep of the serving stream on one warm server: the first ``--count``
     requests submitted as Poisson arrivals at each rate of ``--rates``; per rate the served
     solves/s (count / makespan from first arrival to last completion) and the p50/p99/mean
     latency from submission to completion."""
     from materialite_b200.serving import RVEServer, latency_stats, request_stream, run_stream
-    count = args.count or 32
+    count = args.count or 64
     rates = [float(x) for x in args.rates.split(",")]
     srv = RVEServer(device=0, max_slots=w["slots"], precision="mixed")
     run_stream(srv, request_stream(min(count, 8), 0.0, seed=w["seed"]), timeout=1800)
     out = {"workload": f"serve sweep: {count} requests of the serving stream, "
-                       f"{w['slots']} slots, mixed precision", "rates": []}
+                       f"{w['slots']} slots per class, mixed precision", "rates": []}
     for rate in rates:
-        reqs = request_stream(count, rate, seed=w["seed"])
-        comps, span = run_stream(srv, reqs, timeout=1800)
+        reqs = request_stream(count, rate, seed=w["seed"], workers=host_workers())
+        comps, span = run_stream(srv, reqs, timeout=3600)
         bad = [c.tag for c in comps if c.status != 0]
         if bad:
             raise RuntimeError(f"requests failed: {bad}")
@@ -628,7 +710,10 @@ def main():
         serve_mode(args, w)
         return
     if args.impl == "reference":
-        reference_arm(args, w)
+        if args.workload == "serve":
+            reference_arm(args, w)
+        else:
+            reference_arm_single(args, w)
         return
     from materialite_b200 import replicas
     world, rank, local = replicas.init("nccl")
