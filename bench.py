@@ -65,10 +65,21 @@ WORKLOADS = {
 }
 
 def plane_path(n):
-    """True when the z and y passes of an n^3 float solve run plane-fused (a padded yz
-    plane pair of complex floats fits the 200 KB shared-memory budget)."""
+    """True when the z and y passes of an n^3 float solve run plane-fused: in one block (a
+    padded yz plane pair of complex floats fits the 200 KB shared-memory budget) or split
+    over a thread-block cluster of 2, 4 or 8 blocks, each holding two buffers of its rows'
+    padded z lines (or of its columns' y lines) within the same budget."""
     padded = lambda m: m + (m >> 4) + 1
-    return (2 * padded(n * (n + 2)) + 2 * n) * 8 <= 200 * 1024
+    if (2 * padded(n * (n + 2)) + 2 * n) * 8 <= 200 * 1024:
+        return True
+    hs = n // 2 if n % 2 == 0 else n // 2 + 1
+    for c in (2, 4, 8):
+        if n % c or (2 * hs) % c:
+            continue
+        cap = max(padded(n // c * n), 2 * (n // c) * hs, n * (2 * hs // c))
+        if (2 * cap + 2 * n) * 8 <= 200 * 1024:
+            return True
+    return False
 
 
 # Algorithmic HBM bytes per voxel of each Krylov-iteration kernel with float fields:

@@ -510,7 +510,7 @@ struct Group {
     n += 1;                            // begin
     if (stress_rates) n += 2;          // tangent sum, correction
     n += 2;                            // strain guess, MINRES init
-    const bool plane = plane_ok<double>(plan);
+    const bool plane = three_pass<double>(plan);
     n += plane ? 3 : 5;                // reprojection (mixed) or update (FP64: 1)
     if (plan.fp64) n -= (plane ? 3 : 5) - 1;
     n += 1 + 1;                        // constitutive, stress swap

@@ -61,11 +61,13 @@ struct OccKey {
   int threads;
   size_t smem;
   int dev;
+  int cluster;  // 0: blocks; C: clusters of C blocks
   bool operator<(const OccKey &o) const {
     if (f != o.f) return f < o.f;
     if (threads != o.threads) return threads < o.threads;
     if (smem != o.smem) return smem < o.smem;
-    return dev < o.dev;
+    if (dev != o.dev) return dev < o.dev;
+    return cluster < o.cluster;
   }
 };
 
@@ -73,7 +75,7 @@ static std::mutex g_occ_mutex;
 static std::map<OccKey, int> g_occ;
 
 template <typename F> static int resident_blocks(F f, int threads, size_t smem, int dev) {
-  const OccKey key{(const void *)f, threads, smem, dev};
+  const OccKey key{(const void *)f, threads, smem, dev, 0};
   {
     std::lock_guard<std::mutex> lk(g_occ_mutex);
     auto it = g_occ.find(key);
@@ -95,11 +97,64 @@ static int persistent_grid(F f, int threads, size_t smem, long long items, int d
   return (int)std::max(1LL, std::min<long long>(items, resident_blocks(f, threads, smem, dev)));
 }
 
+// Clusters of C blocks resident at once (a cluster must fit the SMs of one GPC).
+template <typename... A>
+static int resident_clusters(void (*f)(A...), int C, int threads, size_t smem, int dev) {
+  const OccKey key{(const void *)f, threads, smem, dev, C};
+  {
+    std::lock_guard<std::mutex> lk(g_occ_mutex);
+    auto it = g_occ.find(key);
+    if (it != g_occ.end()) return it->second;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(C);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, f, &cfg) != cudaSuccess || n < 1) n = 1;
+  cudaGetLastError();
+  std::lock_guard<std::mutex> lk(g_occ_mutex);
+  g_occ[key] = n;
+  return n;
+}
+
+// Persistent launch of a cluster kernel: as many clusters as are resident at once, but no
+// more than there are items.
+template <typename... P, typename... A>
+static int launch_clustered(void (*f)(P...), int C, size_t smem, long long items, int dev,
+                            cudaStream_t stream, A &&...args) {
+  const int ncl = (int)std::max(1LL, std::min<long long>(items, resident_clusters(f, C, CLUSTER_THREADS, smem, dev)));
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3((unsigned)(ncl * C));
+  cfg.blockDim = dim3(CLUSTER_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, f, std::forward<A>(args)...);
+  if (e != cudaSuccess)
+    return ssfft_internal_fail(SSFFT_E_CUDA, std::string("cluster launch: ") + cudaGetErrorString(e));
+  return 0;
+}
+
 // ---------------------------------------------------------------------------------------
 // grid plan
 // ---------------------------------------------------------------------------------------
 static const size_t SMEM_LIMIT = 200 * 1024;
 #define PLANE_SMEM_LIMIT (200 * 1024)
+#define CLUSTER_MAX 8  // largest portable cluster
 #define MAX_ITEMS_PER_SLOT 65536
 
 struct GridPlan {
@@ -175,6 +230,38 @@ template <typename T> static void fill_grid(GridPlan &p) {
 
 template <typename T> static bool plane_ok(const GridPlan &p) {
   return p.use_plane && smem_plane_bytes<T>(p.ny, p.nz) <= PLANE_SMEM_LIMIT;
+}
+
+// Blocks per cluster of the cluster plane passes (0: not used): the smallest C in 2, 4, 8
+// whose blocks fit the shared-memory budget, for grids whose plane does not fit one block.
+// SSFFT_CLUSTER=C asks for a larger C where it divides the plane.
+template <typename T> static int cluster_size(const GridPlan &p) {
+  if (!p.use_plane || plane_ok<T>(p)) return 0;
+  const int hs = (p.nz % 2 == 0) ? p.nz / 2 : p.hz;
+  const char *env = getenv("SSFFT_CLUSTER");
+  const int want = env ? atoi(env) : 0;
+  for (int C = 2; C <= CLUSTER_MAX; C *= 2) {
+    if (p.ny % C != 0 || (2 * hs) % C != 0 || C < want) continue;
+    if (smem_cplane_bytes<T>(p.ny, p.nz, hs, C) <= PLANE_SMEM_LIMIT) return C;
+  }
+  return 0;
+}
+
+template <typename T> static ClusterGeo cluster_geo(const GridPlan &p, int C) {
+  ClusterGeo q;
+  const int hs = (p.nz % 2 == 0) ? p.nz / 2 : p.hz;
+  q.C = C;
+  q.R = p.ny / C;
+  q.Lq = 2 * hs / C;
+  q.cap = cplane_buf_elems(p.ny, p.nz, hs, C);
+  q.fd_R = make_fastdiv((uint32_t)q.R);
+  q.fd_Lq = make_fastdiv((uint32_t)q.Lq);
+  return q;
+}
+
+// The projection runs as three passes (z and y fused, in one block or one cluster).
+template <typename T> static bool three_pass(const GridPlan &p) {
+  return plane_ok<T>(p) || cluster_size<T>(p) > 0;
 }
 
 // Threads of a plane block: 1024 when a single block fits an SM (228 KB of shared memory),
@@ -274,7 +361,7 @@ static int plan_create(GridPlan &p, const ssfft_config *cfg, cudaStream_t stream
   const Grid<double> &g = p.gd;
   size_t need = 0;
   need = std::max(need, (size_t)3 * items_z(g));
-  need = std::max(need, (size_t)3 * items_plane(g));
+  need = std::max(need, (size_t)3 * CLUSTER_MAX * items_plane(g));
   need = std::max(need, (size_t)NORM_VALS * norm_items(p.V));
   need = std::max(need, (size_t)21 * vec_items(p.V));
   need = std::max(need, (size_t)vec_items(6 * p.V));
@@ -311,6 +398,21 @@ template <typename T, typename TF, int PT> static int plane_attrs(int m) {
   return 0;
 }
 
+template <typename T, typename TF> static int cluster_attrs(int m) {
+  CKR(smem_attr(zyfwd_cl_kernel<T, TF, PRO_INPUT>, m));
+  CKR(smem_attr(zyfwd_cl_kernel<T, TF, PRO_RESIDUAL>, m));
+  CKR(smem_attr(zyfwd_cl_kernel<T, TF, PRO_REPROJECT>, m));
+  CKR(smem_attr(yzinv_cl_kernel<T, TF, EPI_STORE>, m));
+  CKR(smem_attr(yzinv_cl_kernel<T, TF, EPI_RESIDUAL>, m));
+  CKR(smem_attr(yzinv_cl_kernel<T, TF, EPI_REPROJECT>, m));
+  if (sizeof(T) == sizeof(TF)) {
+    CKR(smem_attr(zyfwd_cl_kernel<T, T, PRO_TANGENT_TABLE>, m));
+    CKR(smem_attr(zyfwd_cl_kernel<T, T, PRO_TANGENT_VOXEL>, m));
+    CKR(smem_attr(yzinv_cl_kernel<T, T, EPI_MINRES>, m));
+  }
+  return 0;
+}
+
 // Opt every shared-memory-hungry kernel instantiation into up to `smax` bytes.
 template <typename T, typename TF> static int set_kernel_attrs(size_t smax) {
   const int m = (int)smax;
@@ -328,6 +430,7 @@ template <typename T, typename TF> static int set_kernel_attrs(size_t smax) {
   CKR(smem_attr(zinv_kernel<T, TF, EPI_REPROJECT>, m));
   CKR((plane_attrs<T, TF, 512>(m)));
   CKR((plane_attrs<T, TF, 1024>(m)));
+  CKR((cluster_attrs<T, TF>(m)));
   if (sizeof(T) == sizeof(TF)) {
     CKR(smem_attr(constitutive_kernel<T>, (int)constitutive_smem_bytes()));
     CKR(smem_attr(zfwd_kernel<T, T, PRO_TANGENT_TABLE>, m));
@@ -738,6 +841,21 @@ static int launch_projector(const LaunchCtx &c, const SlotDev<TF> *tab, ExtIO<TF
       auto ki = yzinv_kernel<T, TF, EPI, 512>;
       ki<<<persistent_grid(ki, 512, sp, it, dev), 512, sp, c.stream>>>(g, tab, c.list, io);
     }
+    rec(5);
+    if (c.launches) *c.launches += 3;
+  } else if (const int C = cluster_size<T>(p)) {
+    const ClusterGeo q = cluster_geo<T>(p, C);
+    const size_t sp = smem_cplane_bytes<T>(p.ny, p.nz, g.hs, C);
+    const long long it = (long long)c.cap * items_plane(g);
+    CKR(launch_clustered(zyfwd_cl_kernel<T, TF, PRO>, C, sp, it, dev, c.stream, g, q, tab, c.list, io));
+    rec(1);
+    rec(2);
+    auto kx = xpass_kernel<T, TF, KRY>;
+    kx<<<persistent_grid(kx, XPASS_THREADS, sx, (long long)c.cap * items_x(g), dev), XPASS_THREADS,
+         sx, c.stream>>>(g, tab, c.list);
+    rec(3);
+    rec(4);
+    CKR(launch_clustered(yzinv_cl_kernel<T, TF, EPI>, C, sp, it, dev, c.stream, g, q, tab, c.list, io));
     rec(5);
     if (c.launches) *c.launches += 3;
   } else {

@@ -10,6 +10,9 @@
 //   zinv : complex-to-real inverse along z, then the epilogue
 // Three passes (grids whose yz plane fits in shared memory): zyfwd does z and y of one x
 // plane, yzinv their inverse, and the spectrum crosses HBM four times instead of eight.
+// Larger planes run the same three passes on thread-block clusters (zyfwd_cl, yzinv_cl):
+// the C blocks of a cluster split one plane and exchange it through distributed shared
+// memory between the z and the y transforms.
 //
 // The six real components are paired into three complex lines for the z passes
 // ((0,1), (2,3), (4,5)), so the z transforms run at half length-cost.  Gamma-hat is
@@ -21,6 +24,8 @@
 //
 // Every kernel runs a persistent grid over items (slot, tile); see slots.cuh.
 #pragma once
+
+#include <cooperative_groups.h>
 
 #include "common.cuh"
 #include "fft.cuh"
@@ -795,6 +800,84 @@ template <typename T> inline size_t smem_plane_bytes(int ny, int nz) {
 // hide memory latency with fewer warps), at most 64 registers each.
 #define PLANE_MIN_BLOCKS(PT) ((PT) >= 1024 ? 1 : 2)
 
+// Prologue of a plane item over the points vbase .. vbase + nel - 1 (whole z lines): tau
+// of the component pair p as one complex value per point, into padded z lines in buf.
+template <typename T, typename TF, int PRO>
+__device__ __forceinline__ void plane_prologue(const SlotDev<TF> &S, const ExtIO<TF> &io,
+                                               long long V, long long vbase, int nel, int p,
+                                               const KrylovIn<T, TF> &u, cplx<T> *buf,
+                                               double &xx) {
+  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+    T tau[6];
+    if constexpr (PRO_IS_KRYLOV(PRO)) {
+      tangent_prologue<T, TF, PRO, false>(S, V, vbase + e, u, p, tau, xx);
+      buf[sidx<true>(e)] = mk<T>(tau[0], tau[1]);
+    } else {
+      prologue<T, TF, PRO>(S, io.in, V, vbase + e, tau);
+      buf[sidx<true>(e)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
+    }
+  }
+}
+
+// Epilogue of a plane item: fin holds components 2p (real part) and 2p + 1 (imaginary
+// part) of the points vbase .. vbase + nel - 1 in padded z lines; accumulates the slot's
+// reduction terms.
+template <typename T, typename TF, int EPI>
+__device__ __forceinline__ void plane_epilogue(const SlotDev<TF> &S, const ExtIO<TF> &io,
+                                               long long V, long long vbase, int nel, int p,
+                                               const cplx<T> *fin, double &acc0, double &acc1,
+                                               double &acc2) {
+  KRoles<TF> kr{};
+  T c1 = 0;
+  if constexpr (EPI == EPI_MINRES) {
+    kr = kroles<TF>(S, S.st->itn);
+    c1 = (T)S.st->c_r1;
+  } else if constexpr (EPI == EPI_REPROJECT) {
+    kr = kroles<TF>(S, 0);
+  }
+  if constexpr (EPI == EPI_MINRES) {
+    // batches of EPI_BATCH elements per thread: all r1 / r2 loads before the y' stores
+    constexpr int B = EPI_BATCH;
+    const long long o0 = (2 * p) * V, o1 = (2 * p + 1) * V;
+    for (int e0 = threadIdx.x; e0 < nel; e0 += B * blockDim.x) {
+      T l0[B], l1[B], m0[B], m1[B];
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        const int e = e0 + b * blockDim.x;
+        if (e < nel) {
+          const long long v = vbase + e;
+          l0[b] = (T)kr.P[o0 + v];
+          l1[b] = (T)kr.P[o1 + v];
+          m0[b] = (T)kr.Q[o0 + v];
+          m1[b] = (T)kr.Q[o1 + v];
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        const int e = e0 + b * blockDim.x;
+        if (e < nel) {
+          const long long v = vbase + e;
+          const cplx<T> Z = fin[sidx<true>(e)];
+          const T y0 = Z.x - c1 * l0[b];
+          const T y1 = Z.y - c1 * l1[b];
+          kr.Y[o0 + v] = (TF)y0;
+          kr.Y[o1 + v] = (TF)y1;
+          acc0 += (double)m0[b] * (double)y0 + (double)m1[b] * (double)y1;
+          acc1 += (double)y0 * (double)y0 + (double)y1 * (double)y1;
+          acc2 += (double)m0[b] * (double)m0[b] + (double)m1[b] * (double)m1[b];
+        }
+      }
+    }
+  } else {
+    for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+      const cplx<T> Z = fin[sidx<true>(e)];
+      const T r[2] = {Z.x, Z.y};
+      epilogue_point<T, TF, EPI, 2>(S, io, kr, c1, V, vbase + e, 2 * p, r, nullptr, nullptr,
+                                    acc0, acc1, acc2);
+    }
+  }
+}
+
 template <typename T, typename TF, int PRO, int PT>
 __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     zyfwd_kernel(Grid<T> g, const SlotDev<TF> *__restrict__ tab, SlotList list, ExtIO<TF> io) {
@@ -825,16 +908,7 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     double xx = 0.0;
     const long long vbase = (long long)x * ny * nz;
     __syncthreads();
-    for (int e = threadIdx.x; e < ny * nz; e += blockDim.x) {
-      T tau[6];
-      if constexpr (PRO_IS_KRYLOV(PRO)) {
-        tangent_prologue<T, TF, PRO, false>(S, V, vbase + e, u, p, tau, xx);
-        bufA[sidx<true>(e)] = mk<T>(tau[0], tau[1]);
-      } else {
-        prologue<T, TF, PRO>(S, io.in, V, vbase + e, tau);
-        bufA[sidx<true>(e)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
-      }
-    }
+    plane_prologue<T, TF, PRO>(S, io, V, vbase, ny * nz, p, u, bufA, xx);
     __syncthreads();
     const LineLayout Lz(ny, ny, 0, nz, 1, g.fd_ny, g.fd_ny);
     cplx<T> *res = smem_fft<T, false, false, true>(bufA, bufB, Lz, g.pz, twz);
@@ -912,58 +986,203 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     const LineLayout Lz(ny, ny, 0, nz, 1, g.fd_ny, g.fd_ny);
     cplx<T> *fin = smem_fft<T, true, false, true>(oth, res, Lz, g.pz, twz);
     double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-    const long long vbase = (long long)x * ny * nz;
-    const int nel = ny * nz;
-    KRoles<TF> kr{};
-    T c1 = 0;
-    if constexpr (EPI == EPI_MINRES) {
-      kr = kroles<TF>(S, S.st->itn);
-      c1 = (T)S.st->c_r1;
-    } else if constexpr (EPI == EPI_REPROJECT) {
-      kr = kroles<TF>(S, 0);
-    }
-    if constexpr (EPI == EPI_MINRES) {
-      // batches of EPI_BATCH elements per thread: all r1 / r2 loads before the y' stores
-      constexpr int B = EPI_BATCH;
-      const long long o0 = (2 * p) * V, o1 = (2 * p + 1) * V;
-      for (int e0 = threadIdx.x; e0 < nel; e0 += B * blockDim.x) {
-        T l0[B], l1[B], m0[B], m1[B];
-#pragma unroll
-        for (int b = 0; b < B; ++b) {
-          const int e = e0 + b * blockDim.x;
-          if (e < nel) {
-            const long long v = vbase + e;
-            l0[b] = (T)kr.P[o0 + v];
-            l1[b] = (T)kr.P[o1 + v];
-            m0[b] = (T)kr.Q[o0 + v];
-            m1[b] = (T)kr.Q[o1 + v];
-          }
-        }
-#pragma unroll
-        for (int b = 0; b < B; ++b) {
-          const int e = e0 + b * blockDim.x;
-          if (e < nel) {
-            const long long v = vbase + e;
-            const cplx<T> Z = fin[sidx<true>(e)];
-            const T y0 = Z.x - c1 * l0[b];
-            const T y1 = Z.y - c1 * l1[b];
-            kr.Y[o0 + v] = (TF)y0;
-            kr.Y[o1 + v] = (TF)y1;
-            acc0 += (double)m0[b] * (double)y0 + (double)m1[b] * (double)y1;
-            acc1 += (double)y0 * (double)y0 + (double)y1 * (double)y1;
-            acc2 += (double)m0[b] * (double)m0[b] + (double)m1[b] * (double)m1[b];
-          }
-        }
-      }
-    } else {
-      for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-        const cplx<T> Z = fin[sidx<true>(e)];
-        const T r[2] = {Z.x, Z.y};
-        epilogue_point<T, TF, EPI, 2>(S, io, kr, c1, V, vbase + e, 2 * p, r, nullptr, nullptr,
-                                      acc0, acc1, acc2);
-      }
-    }
+    plane_epilogue<T, TF, EPI>(S, io, V, (long long)x * ny * nz, ny * nz, p, fin, acc0, acc1, acc2);
     finish_inverse<TF, EPI>(S, acc0, acc1, acc2, local, per, red);
+    __syncthreads();
+  }
+}
+
+// ---- cluster plane passes (planes that fit the shared memory of a block cluster) ---------
+//
+// C blocks (a thread-block cluster) share one (x plane, pair) item.  Block r transforms
+// the R = ny / C rows y in [rR, rR + R) along z, and along y the Lq = 2 hs / C half-spectrum
+// columns with c hs + kz in [r Lq, r Lq + Lq) (c: component 2p + c of the pair).  Between
+// the two transforms each block stores its split half spectra straight into the owning
+// block's shared memory (distributed shared memory: no round trip through HBM or L2), and
+// the inverse does the same in reverse.  Two cluster barriers per item order the exchange:
+// the first finds every block's free buffer free, the second finds the exchange complete.
+// Every block of a cluster runs the same items and reaches every barrier, also for an item
+// it skips; the buffer that takes the exchange follows from the stage count of the
+// transform before it, not from whether the block ran it.
+struct ClusterGeo {
+  int C, R, Lq, cap;  // cluster size, rows and columns per block, elements per buffer
+  FastDiv fd_R, fd_Lq;
+};
+
+// Elements of one buffer: R padded z lines, the split half spectra of R rows (2 R hs), or
+// the Lq columns of ny points a block transforms along y.
+__host__ __device__ inline int cplane_buf_elems(int ny, int nz, int hs, int C) {
+  const int R = ny / C, Lq = 2 * hs / C;
+  int n = padded_len(R * nz);
+  n = n > 2 * R * hs ? n : 2 * R * hs;
+  return n > ny * Lq ? n : ny * Lq;
+}
+template <typename T> inline size_t smem_cplane_bytes(int ny, int nz, int hs, int C) {
+  return (2 * (size_t)cplane_buf_elems(ny, nz, hs, C) + ny + nz) * sizeof(cplx<T>);
+}
+
+#define CLUSTER_THREADS 1024
+
+template <typename T, typename TF, int PRO>
+__global__ void __launch_bounds__(CLUSTER_THREADS, 1)
+    zyfwd_cl_kernel(Grid<T> g, ClusterGeo cq, const SlotDev<TF> *__restrict__ tab,
+                    SlotList list, ExtIO<TF> io) {
+  namespace cg = cooperative_groups;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[32];
+  __shared__ __align__(16) unsigned char sdesc[sizeof(SlotDev<TF>)];
+  cg::cluster_group cl = cg::this_cluster();
+  const int C = cq.C, R = cq.R, Lq = cq.Lq;
+  const int rank = (int)cl.block_rank();
+  const int ny = g.ny, nz = g.nz, hs = g.hs;
+  const long long V = g.V;
+  cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
+  cplx<T> *bufB = bufA + cq.cap;
+  cplx<T> *twy = bufB + cq.cap;
+  cplx<T> *twz = twy + ny;
+  load_table<T>(twy, g.twy, ny);
+  load_table<T>(twz, g.twz, nz);
+  // after the z transform the result is in bufA for an even stage count
+  cplx<T> *res = (g.pz.nrad & 1) ? bufB : bufA;
+  cplx<T> *oth = (g.pz.nrad & 1) ? bufA : bufB;
+  const int per = items_plane(g);
+  const int n_items = list_items(list, per);
+  const int plane = ny * hs;
+  const int y0 = rank * R;
+  const int cown = (rank * Lq) / hs, k0 = rank * Lq - cown * hs;  // owned columns
+  const int ncl = gridDim.x / C;
+  for (int item = blockIdx.x / C; item < n_items; item += ncl) {
+    const int k = udiv(item, g.fd_it_plane);
+    const int local = item - k * per;
+    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc);
+    const bool skip = skip_item<TF, PRO>(S);
+    const int x = udiv(local, g.fd_3);
+    const int p = local - 3 * x;
+    KrylovIn<T, TF> u{};
+    if constexpr (PRO_IS_KRYLOV(PRO)) u = krylov_in<T, TF>(S);
+    double xx = 0.0;
+    if (!skip) {
+      __syncthreads();
+      plane_prologue<T, TF, PRO>(S, io, V, ((long long)x * ny + y0) * nz, R * nz, p, u, bufA, xx);
+      __syncthreads();
+      const LineLayout Lz(R, R, 0, nz, 1, cq.fd_R, cq.fd_R);
+      smem_fft<T, false, false, true>(bufA, bufB, Lz, g.pz, twz);
+    }
+    cl.sync();  // every block's z transform is done: its other buffer is free
+    if (!skip) {
+      // split the paired transform; column (c, kz) goes to block (c hs + kz) / Lq, which
+      // holds it at [y][column - its first column]
+      for (int e = threadIdx.x; e < R * hs; e += blockDim.x) {
+        const int yl = udiv(e, g.fd_hs), kk = e - yl * hs;
+        const cplx<T> Z = res[sidx<true>(yl * nz + kk)];
+        const cplx<T> Zm = res[sidx<true>(yl * nz + (kk == 0 ? 0 : nz - kk))];
+        const cplx<T> A = mk<T>((T)0.5 * (Z.x + Zm.x), (T)0.5 * (Z.y - Zm.y));
+        const cplx<T> B = mk<T>((T)0.5 * (Z.y + Zm.y), (T)0.5 * (Zm.x - Z.x));
+        const int qa = udiv(kk, cq.fd_Lq), qb = udiv(hs + kk, cq.fd_Lq);
+        cplx<T> *da = cl.map_shared_rank(oth, qa);
+        cplx<T> *db = cl.map_shared_rank(oth, qb);
+        da[(y0 + yl) * Lq + (kk - qa * Lq)] = A;
+        db[(y0 + yl) * Lq + (hs + kk - qb * Lq)] = B;
+      }
+    }
+    cl.sync();  // the owned columns are complete
+    if (!skip) {
+      const LineLayout Ly(Lq, Lq, 0, 1, Lq, cq.fd_Lq, cq.fd_Lq);
+      cplx<T> *out = smem_fft<T, false, true>(oth, res, Ly, g.py, twy);
+      cplx<T> *spec = reinterpret_cast<cplx<T> *>(S.spec) + (2 * p + cown) * g.S +
+                      (long long)x * plane + k0;
+      for (int e = threadIdx.x; e < ny * Lq; e += blockDim.x) {
+        const int y = udiv(e, cq.fd_Lq), kl = e - y * Lq;
+        spec[(long long)y * hs + kl] = out[e];
+      }
+      if constexpr (PRO_IS_KRYLOV(PRO)) {
+        if (u.on) finish_pending_update(S, xx, local * C + rank, per * C, red);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T, typename TF, int EPI>
+__global__ void __launch_bounds__(CLUSTER_THREADS, 1)
+    yzinv_cl_kernel(Grid<T> g, ClusterGeo cq, const SlotDev<TF> *__restrict__ tab,
+                    SlotList list, ExtIO<TF> io) {
+  namespace cg = cooperative_groups;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[32];
+  __shared__ __align__(16) unsigned char sdesc[sizeof(SlotDev<TF>)];
+  cg::cluster_group cl = cg::this_cluster();
+  const int C = cq.C, R = cq.R, Lq = cq.Lq;
+  const int rank = (int)cl.block_rank();
+  const int ny = g.ny, nz = g.nz, hz = g.hz, hs = g.hs;
+  const long long V = g.V;
+  cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
+  cplx<T> *bufB = bufA + cq.cap;
+  cplx<T> *twy = bufB + cq.cap;
+  cplx<T> *twz = twy + ny;
+  load_table<T>(twy, g.twy, ny);
+  load_table<T>(twz, g.twz, nz);
+  // after the y transform the result is in bufA for an even stage count
+  cplx<T> *res = (g.py.nrad & 1) ? bufB : bufA;
+  cplx<T> *oth = (g.py.nrad & 1) ? bufA : bufB;
+  const int per = items_plane(g);
+  const int n_items = list_items(list, per);
+  const int plane = ny * hs;
+  const int y0 = rank * R;
+  const int lam0 = rank * Lq;
+  const int cown = lam0 / hs, k0 = lam0 - cown * hs;
+  const int ncl = gridDim.x / C;
+  for (int item = blockIdx.x / C; item < n_items; item += ncl) {
+    const int k = udiv(item, g.fd_it_plane);
+    const int local = item - k * per;
+    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc);
+    const bool skip = (EPI == EPI_MINRES) && block_read_flag(&S.st->done);
+    const int x = udiv(local, g.fd_3);
+    const int p = local - 3 * x;
+    if (!skip) {
+      const cplx<T> *spec = reinterpret_cast<const cplx<T> *>(S.spec) + (2 * p + cown) * g.S +
+                            (long long)x * plane + k0;
+      __syncthreads();
+      for (int e = threadIdx.x; e < ny * Lq; e += blockDim.x) {
+        const int y = udiv(e, cq.fd_Lq), kl = e - y * Lq;
+        bufA[e] = spec[(long long)y * hs + kl];
+      }
+      __syncthreads();
+      const LineLayout Ly(Lq, Lq, 0, 1, Lq, cq.fd_Lq, cq.fd_Lq);
+      smem_fft<T, true, true>(bufA, bufB, Ly, g.py, twy);
+    }
+    cl.sync();  // every block's y transform is done: its other buffer is free
+    if (!skip) {
+      // row y goes to block y / R, which holds the half spectra of its rows at [c][y][kz]
+      for (int e = threadIdx.x; e < ny * Lq; e += blockDim.x) {
+        const int y = udiv(e, cq.fd_Lq), kl = e - y * Lq;
+        const int q = udiv(y, cq.fd_R), yl = y - q * R;
+        const int lam = lam0 + kl;
+        const int c = lam >= hs ? 1 : 0, kk = lam - c * hs;
+        cplx<T> *d = cl.map_shared_rank(oth, q);
+        d[(c * R + yl) * hs + kk] = res[e];
+      }
+    }
+    cl.sync();  // the owned rows are complete
+    if (!skip) {
+      // full z lines of Z = A + iB from the stored halves (Hermitian in z)
+      for (int e = threadIdx.x; e < R * nz; e += blockDim.x) {
+        const int yl = udiv(e, g.fd_nz), kk = e - yl * nz;
+        const bool low = (kk < hz);
+        const int ks = low ? kk : nz - kk;
+        const bool nyq = 2 * ks == nz;  // the unstored Nyquist column is zero
+        const cplx<T> A = nyq ? mk<T>((T)0, (T)0) : oth[yl * hs + ks];
+        const cplx<T> B = nyq ? mk<T>((T)0, (T)0) : oth[(R + yl) * hs + ks];
+        res[sidx<true>(e)] = low ? mk<T>(A.x - B.y, A.y + B.x) : mk<T>(A.x + B.y, B.x - A.y);
+      }
+      __syncthreads();
+      const LineLayout Lz(R, R, 0, nz, 1, cq.fd_R, cq.fd_R);
+      cplx<T> *fin = smem_fft<T, true, false, true>(res, oth, Lz, g.pz, twz);
+      double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+      plane_epilogue<T, TF, EPI>(S, io, V, ((long long)x * ny + y0) * nz, R * nz, p, fin, acc0,
+                                 acc1, acc2);
+      finish_inverse<TF, EPI>(S, acc0, acc1, acc2, local * C + rank, per * C, red);
+    }
     __syncthreads();
   }
 }

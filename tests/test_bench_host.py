@@ -12,14 +12,16 @@ from materialite_b200.serving import request_stream
 
 
 def test_plane_path_rule():
-    assert [bench.plane_path(n) for n in (32, 48, 64, 96, 128)] == [True] * 4 + [False]
+    # one block up to 96^3; clusters of 2 (128^3) and 8 (256^3) blocks; nothing at 512^3
+    assert [bench.plane_path(n) for n in (32, 48, 64, 96, 128, 256, 512)] == [True] * 6 + [False]
 
 
 def test_byte_model():
     b128 = bench.kernel_bytes_per_voxel(128)
     spec = 6 * 64 / 128 * 8.0  # the Nyquist column of an even grid is not stored
     assert b128["zfwd"] == pytest.approx(8 * 24 + 4 + spec)
-    assert b128["yfwd"] == pytest.approx(2 * spec) and b128["update"] == 0.0
+    assert b128["yfwd"] == 0.0 and b128["update"] == 0.0
+    assert bench.kernel_bytes_per_voxel(512)["yfwd"] == pytest.approx(2 * 6 * 256 / 512 * 8.0)
     b64 = bench.kernel_bytes_per_voxel(64, table_mode=False)
     assert b64["yfwd"] == 0.0 and b64["zfwd"] == pytest.approx(8 * 24 + 84 + 6 * 32 / 64 * 8)
 

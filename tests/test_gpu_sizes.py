@@ -2,8 +2,11 @@
 the C ABI.
 
 * 48^3 and 96^3 carry radix-3 stages (the serving stream's sizes).
-* 96^3 in FP64 and 16x128x128 in float run the five-pass projector because their yz plane
-  does not fit in shared memory, as 128^3 and 256^3 do; 96^3 in float runs plane-fused.
+* 96^3 in FP64 runs the five-pass projector because its yz plane does not fit in shared
+  memory; 96^3 in float runs plane-fused.
+* 128-point yz planes (the plane of the 128^3 workload) and other planes too large for one
+  block run plane-fused on thread-block clusters (2 blocks in float, 4 in FP64 at 128x128;
+  SSFFT_CLUSTER asks for larger clusters), and on the five-pass projector.
 * Crystal plasticity at 32^3 (the smallest serving size) on both projector paths.
 * One case with CUDA graphs off (SSFFT_NO_GRAPHS=1): every Krylov kernel launched from the
   host.
@@ -142,14 +145,59 @@ def test_elastic_96(precision, tol):
         assert_counts_close(st, ost)
 
 
+def use_cluster(monkeypatch, path):
+    """plane: the default plane-fused path (clusters where one block cannot hold the
+    plane); clusterN: clusters of at least N blocks; five_pass: no plane fusion."""
+    monkeypatch.delenv("SSFFT_CLUSTER", raising=False)
+    use_path(monkeypatch, "five_pass" if path == "five_pass" else "plane")
+    if path.startswith("cluster"):
+        monkeypatch.setenv("SSFFT_CLUSTER", path[len("cluster"):])
+
+
+@pytest.mark.parametrize("path", ["plane", "cluster8", "five_pass"])
+@pytest.mark.parametrize("dims", [(4, 128, 128), (3, 128, 135), (2, 144, 120)])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 3e-6)])
+def test_cluster_projection(dims, precision, tol, path, monkeypatch):
+    """The projection on planes too large for one block: 128x128 (the 128^3 workload's
+    plane), an odd z length (135 = 3^3 5, 68 stored columns) and 144x120 (radix 3 along y,
+    radix 3 and 5 along z), against the oracle's Gamma-hat."""
+    use_cluster(monkeypatch, path)
+    V = int(np.prod(dims))
+    mask = [0, 1, 1, 1, 1, 1]
+    tau = np.random.default_rng(11).standard_normal((V, 6))
+    h = SolverHandle(dims, mask, precision)
+    try:
+        out = h.apply_projection(tau)
+    finally:
+        h.close()
+    ref = O.apply_projection(O.projection_operator(dims, mask), tau)
+    assert rel_l2(out, ref) < tol
+
+
+@pytest.mark.parametrize("path", ["plane", "cluster4", "five_pass"])
 @pytest.mark.parametrize("dims", [(16, 128, 128), (128, 32, 32)])
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-5)])
-def test_elastic_128_axes(dims, precision, tol):
-    """128-point axes: 16x128x128 runs the five-pass projector in both precisions (its
-    128x128 yz plane is the plane of the 128^3 workload); 128x32x32 has the 128-point x
-    pass of that workload."""
+def test_elastic_128_axes(dims, precision, tol, path, monkeypatch):
+    """128-point axes: 16x128x128 has the 128x128 yz plane of the 128^3 workload (cluster
+    passes, or five passes); 128x32x32 has the 128-point x pass of that workload."""
+    use_cluster(monkeypatch, path)
     R, ref, ost = elastic_reference(dims, 2)
     out, st = run_elastic(dims, R, 2, precision)
+    assert rel_l2(out["stress"], ref["stress"]) < tol
+    assert rel_l2(out["strain"], ref["strain"]) < tol
+    if precision == "fp64":
+        assert_counts_close(st, ost)
+
+
+@pytest.mark.parametrize("path", ["plane", "five_pass"])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-6), ("mixed", 1e-5)])
+def test_evp_cluster(precision, tol, path, monkeypatch):
+    """Crystal plasticity (per-point tangents) on a 4x128x128 grid: the Krylov passes with
+    the per-voxel tangent on the cluster path, two load steps past the onset of slip."""
+    use_cluster(monkeypatch, path)
+    dims = (4, 128, 128)
+    R, ref = evp_reference(dims, 2)
+    out = run_evp(dims, R, 2, precision)
     assert rel_l2(out["stress"], ref["stress"]) < tol
     assert rel_l2(out["strain"], ref["strain"]) < tol
 
