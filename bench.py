@@ -642,6 +642,9 @@ def accuracy_mode(args, w):
                      "mean_stress_xx": float(res["stress"][:, 0].mean())}
         h.close()
         print(json.dumps({prec: out[prec]}), flush=True)
+        # per attempted increment: t, dt, converged, Newton, Krylov, eq. error, max
+        # constitutive iterations (where the two precisions part ways)
+        print(json.dumps({prec + "_attempts": st.attempts}), flush=True)
     a, b = stress["mixed"], stress["fp64"]
     out["stress_rel_l2_mixed_vs_fp64"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
     print(json.dumps(out), flush=True)

@@ -1,22 +1,23 @@
 // Batched solves: a group holds up to B RVE requests of one grid size, precision and
-// tangent kind (table or per-voxel) as slots, and advances all of them together.  One
-// "round" gives every live slot one unit of the reference's Newton loop
-// (small_strain_fft.py:106-246):
+// tangent kind (table or per-voxel) as slots, and advances all of them together through the
+// reference's time and Newton loops (small_strain_fft.py:106-246), each slot at its own
+// pace.  One pass of the device loop is
 //
-//   slot starting a load increment (FRESH): strain guess, constitutive call, residual,
-//     norms -- the it == 1 prologue of :130-146;
-//   slot in its Newton loop (SOLVE): MINRES solve (:151), strain update (:154-155),
-//     constitutive call, residual, norms and the convergence tests (:157-211).
+//   schedule: slots whose MINRES solve finished and slots starting a load increment are
+//     listed for service;
+//   service (a conditional subgraph, skipped when the list is empty): for a finished solve
+//     the strain update (:154-155); for an increment start the strain guess (:108-123);
+//     then, for all listed slots, the constitutive call, the residual and the norms
+//     (:130-146, :157-200), and the per-slot decisions -- convergence tests, the commit
+//     (as role swaps) with the dt update of _get_new_time_increment (:266-279), the
+//     cutback of :242-246 -- and the start of the next MINRES solve (:151);
+//   one Krylov chunk over every slot whose solve is live (MINRES, :281-299);
 //
-// Every kernel of a round covers all listed slots at once (slot lists, slots.cuh), and the
-// Krylov loop runs until the last slot's MINRES is done, slots dropping out of the active
-// list as they finish.  group_decide_kernel then applies, per slot and on the device, the
-// reference's convergence tests, the commit (as role swaps) with the dt update of
-// _get_new_time_increment (:266-279), and the cutback of :242-246, and picks each slot's
-// next state.  Rounds repeat in a CUDA-graph while node until a slot finishes its solve
-// (the host then hands its result back and may load a new request into the slot); the
-// Krylov loop inside a round is a nested while node.  No host round trip happens per
-// Newton iteration.
+// so a slot never waits for another slot's solve: a slot whose solve finishes is served
+// at the next pass while the others keep iterating.  The passes repeat in a CUDA-graph
+// while node until a slot finishes its whole solve (the host then hands its result back and
+// may load a new request into the slot) or the host raises the group's wake flag (a
+// request waits for a free slot).  No host round trip happens per Newton iteration.
 #pragma once
 
 #include <memory>
@@ -36,60 +37,95 @@ struct GroupCtl {
   double mean_stress[6], mean_strain[6];
 };
 
-// Slot lists of a round.
-enum { GL_FRESH = 0, GL_SOLVE, GL_KRY, GL_NEWTON, GL_TSUM, GL_COMMIT, GL_COUNT };
+// Slot lists of the loop: KRY (live MINRES solves; kept across passes), and the lists of
+// one service: FRESH (increment starts), TAIL (finished solves), NEWTON (both), TSUM
+// (increment starts under a stress increment), COMMIT (slots committed by the last
+// service: slip resistances to copy), ENTER (slots that start a MINRES solve).
+enum { GL_KRY = 0, GL_FRESH, GL_TAIL, GL_NEWTON, GL_TSUM, GL_COMMIT, GL_ENTER, GL_COUNT };
 
-// Rounds per graph launch at most (a launch also ends when a slot finishes its solve).
-#define GROUP_ROUND_CAP 20000
+// Loop state of a group in device memory: slots finished and passes run since the launch
+// (reset by the host before each launch); passes and services since the group began.
+struct GroupLoop {
+  int finished, pad;
+  unsigned long long launch_passes, passes, services;
+};
 
-// Start of a round: lists of the slots by state, per-increment inputs of the slots that
-// start an increment (load_schedule closures at (t, dt), small_strain_fft.py:108-123), and
-// the Krylov loop's condition.
+// Passes per graph launch at most (a launch also ends when a slot finishes its solve).
+#define GROUP_PASS_CAP 200000
+
+// Per-increment inputs of a slot that starts an increment: the load_schedule closures at
+// (t, dt) (small_strain_fft.py:108-123) and the flags of the strain guess.
+template <typename T> __device__ void group_begin_slot(GroupCtl &c, SlotDev<T> &S) {
+  int imax = 0;
+  bool all_small = true;
+  for (int k = 0; k < 6; ++k) {
+    const double ei = c.er[k] * c.dt;
+    const double si = c.sr[k] * c.dt;
+    S.sv.dEbar[k] = ei;
+    S.sv.dS[k] = si;
+    S.sv.corr[k] = 0.0;
+    S.sbar[k] = c.sr[k] * (c.t + c.dt - c.start_time);
+    if (fabs(ei) > fabs(c.er[imax] * c.dt)) imax = k;
+    if (!(si < 1.0e-14)) all_small = false;
+  }
+  c.max_inc = c.er[imax] * c.dt;
+  S.reset_fluct = (c.max_inc * c.old_max_inc < 0.0) ? 1 : 0;
+  S.first_step = c.step_id == 0 ? 1 : 0;
+  S.fluct_scale = c.pending_scale;
+  c.pending_scale = 1.0;
+  S.dt = c.dt;
+  S.norms_dx = 0;
+  c.newton_it = 0;
+  c.max_cit = 0;
+  c.need_tsum = all_small ? 0 : 1;
+}
+
+// Start of a pass: finished MINRES solves leave the live list (in place, keeping its
+// order) for the tail list; slots in FRESH state are listed for an increment start; the
+// service runs when either list is non-empty.
 template <typename T>
-__global__ void group_begin_kernel(SlotDev<T> *tab, GroupCtl *ctl, int *ids, int *counts, int B,
-                                   cudaGraphConditionalHandle cond_kry, int use_cond) {
+__global__ void group_sched_kernel(SlotDev<T> *tab, GroupCtl *ctl, int *ids, int *counts, int B,
+                                   cudaGraphConditionalHandle cond_srv, int use_cond,
+                                   GroupLoop *loop) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  int n[GL_COUNT] = {0, 0, 0, 0, 0, 0};
-  for (int s = 0; s < B; ++s) {
-    GroupCtl &c = ctl[s];
-    SlotDev<T> &S = tab[s];
-    if (c.state == GS_FRESH) {
-      int imax = 0;
-      bool all_small = true;
-      for (int k = 0; k < 6; ++k) {
-        const double ei = c.er[k] * c.dt;
-        const double si = c.sr[k] * c.dt;
-        S.sv.dEbar[k] = ei;
-        S.sv.dS[k] = si;
-        S.sv.corr[k] = 0.0;
-        S.sbar[k] = c.sr[k] * (c.t + c.dt - c.start_time);
-        if (fabs(ei) > fabs(c.er[imax] * c.dt)) imax = k;
-        if (!(si < 1.0e-14)) all_small = false;
-      }
-      c.max_inc = c.er[imax] * c.dt;
-      S.reset_fluct = (c.max_inc * c.old_max_inc < 0.0) ? 1 : 0;
-      S.first_step = c.step_id == 0 ? 1 : 0;
-      S.fluct_scale = c.pending_scale;
-      c.pending_scale = 1.0;
-      S.dt = c.dt;
-      S.norms_dx = 0;
-      c.newton_it = 0;
-      c.max_cit = 0;
-      c.need_tsum = all_small ? 0 : 1;
-      ids[GL_FRESH * B + n[GL_FRESH]++] = s;
-      ids[GL_NEWTON * B + n[GL_NEWTON]++] = s;
-      if (c.need_tsum) ids[GL_TSUM * B + n[GL_TSUM]++] = s;
-      for (int k = 0; k < 4; ++k) S.citers[k] = 0;
-    } else if (c.state == GS_SOLVE) {
+  int n[GL_COUNT];
+  for (int l = 0; l < GL_COUNT; ++l) n[l] = 0;
+  int *kry = ids + GL_KRY * B;
+  const int nk = counts[GL_KRY];
+  for (int k = 0; k < nk; ++k) {
+    const int s = kry[k];
+    minres_cap(tab[s].st);
+    if (tab[s].st->done) {
+      SlotDev<T> &S = tab[s];
       S.norms_dx = 1;
-      ids[GL_SOLVE * B + n[GL_SOLVE]++] = s;
-      ids[GL_KRY * B + n[GL_KRY]++] = s;
-      ids[GL_NEWTON * B + n[GL_NEWTON]++] = s;
-      for (int k = 0; k < 4; ++k) S.citers[k] = 0;
+      for (int q = 0; q < 4; ++q) S.citers[q] = 0;
+      ids[GL_TAIL * B + n[GL_TAIL]++] = s;
+    } else {
+      kry[n[GL_KRY]++] = s;
     }
   }
-  for (int l = 0; l < GL_COUNT; ++l) counts[l] = n[l];  // the commit list is consumed
-  if (use_cond) cudaGraphSetConditional(cond_kry, n[GL_SOLVE] > 0 ? 1u : 0u);
+  for (int s = 0; s < B; ++s) {
+    GroupCtl &c = ctl[s];
+    if (c.state != GS_FRESH) continue;
+    SlotDev<T> &S = tab[s];
+    group_begin_slot<T>(c, S);
+    for (int q = 0; q < 4; ++q) S.citers[q] = 0;
+    ids[GL_FRESH * B + n[GL_FRESH]++] = s;
+    if (c.need_tsum) ids[GL_TSUM * B + n[GL_TSUM]++] = s;
+  }
+  // NEWTON = FRESH then TAIL
+  for (int k = 0; k < n[GL_FRESH]; ++k) ids[GL_NEWTON * B + n[GL_NEWTON]++] = ids[GL_FRESH * B + k];
+  for (int k = 0; k < n[GL_TAIL]; ++k) ids[GL_NEWTON * B + n[GL_NEWTON]++] = ids[GL_TAIL * B + k];
+  counts[GL_KRY] = n[GL_KRY];
+  counts[GL_FRESH] = n[GL_FRESH];
+  counts[GL_TAIL] = n[GL_TAIL];
+  counts[GL_NEWTON] = n[GL_NEWTON];
+  counts[GL_TSUM] = n[GL_TSUM];
+  counts[GL_ENTER] = 0;
+  loop->passes += 1;
+  loop->launch_passes += 1;
+  if (n[GL_NEWTON] > 0) loop->services += 1;
+  if (use_cond) cudaGraphSetConditional(cond_srv, n[GL_NEWTON] > 0 ? 1u : 0u);
 }
 
 // strain += tangent.mean().inv @ stress_increment (small_strain_fft.py:119-120) for the
@@ -144,14 +180,16 @@ __device__ inline void group_cutback(GroupCtl &c) {
   }
 }
 
-// End of a round: the Newton decisions of every listed slot; the rounds loop continues
-// while slots are live and none has finished.  counters[0] counts rounds.
+// End of a service: the Newton decisions of every listed slot.  A slot that goes on
+// solving (an increment start whose residual is known, or a Newton iteration that did not
+// converge) is listed to start a MINRES solve and joins the live list; a committed slot
+// starts its next increment at the next service.
 template <typename T>
 __global__ void group_decide_kernel(SlotDev<T> *tab, GroupCtl *ctl, int *ids, int *counts,
-                                    int B, long long V, cudaGraphConditionalHandle cond_round,
-                                    int use_cond, unsigned long long *counters) {
+                                    int B, long long V, GroupLoop *loop) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  int finished = 0, n_commit = 0;
+  int n_commit = 0, n_enter = 0, finished = 0;
+  int nk = counts[GL_KRY];
   for (int k = 0; k < counts[GL_NEWTON]; ++k) {
     const int s = ids[GL_NEWTON * B + k];
     GroupCtl &c = ctl[s];
@@ -167,6 +205,7 @@ __global__ void group_decide_kernel(SlotDev<T> *tab, GroupCtl *ctl, int *ids, in
       S.g_out = t;
     }
     const double *r = S.results;
+    bool solve = false;
     if (c.state == GS_FRESH) {
       if (cf) {
         group_cutback(c);
@@ -176,8 +215,9 @@ __global__ void group_decide_kernel(SlotDev<T> *tab, GroupCtl *ctl, int *ids, in
         c.eq_err = r[40] / c.mvm;
         c.old_eq = fmax(c.eq_err, c.gtol);
         c.state = GS_SOLVE;
+        solve = true;
       }
-    } else {  // GS_SOLVE
+    } else {  // GS_SOLVE, its MINRES solve finished
       c.newton_it += 1;
       c.newton_total += 1;
       c.krylov_total += S.st->itn;
@@ -236,21 +276,38 @@ __global__ void group_decide_kernel(SlotDev<T> *tab, GroupCtl *ctl, int *ids, in
           group_cutback(c);
         } else {
           c.old_eq = fmax(c.eq_err, c.gtol);
+          solve = true;
         }
       }
+    }
+    if (solve) {
+      ids[GL_ENTER * B + n_enter++] = s;
+      ids[GL_KRY * B + nk++] = s;
     }
     if (c.state == GS_DONE || c.state == GS_FAILED) ++finished;
   }
   counts[GL_COMMIT] = n_commit;
+  counts[GL_ENTER] = n_enter;
+  counts[GL_KRY] = nk;
+  loop->finished += finished;
+}
+
+// End of a pass: the loop goes on while a slot is live, none has finished since the
+// launch, the host has not asked for the device (a request waits for a free slot), and the
+// pass cap is not reached.
+__global__ void group_loop_kernel(const GroupCtl *ctl, int B, GroupLoop *loop,
+                                  const volatile int *wake, cudaGraphConditionalHandle cond_loop,
+                                  int use_cond) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
   int live = 0;
   for (int s = 0; s < B; ++s)
     if (ctl[s].state == GS_FRESH || ctl[s].state == GS_SOLVE) ++live;
-  counters[0] += 1;
-  const bool more = live > 0 && finished == 0 && counters[0] % GROUP_ROUND_CAP != 0;
-  if (use_cond) cudaGraphSetConditional(cond_round, more ? 1u : 0u);
+  const bool more = live > 0 && loop->finished == 0 && *wake == 0 &&
+                    loop->launch_passes < GROUP_PASS_CAP;
+  if (use_cond) cudaGraphSetConditional(cond_loop, more ? 1u : 0u);
 }
 
-// Krylov chunk of a group: iterations between looks at the slots' MINRES states.
+// Krylov iterations per pass (between looks at the slots' MINRES states).
 #define GROUP_KRYLOV_CHUNK 4
 
 // ---------------------------------------------------------------------------------------
@@ -271,11 +328,14 @@ struct Group {
   GroupCtl *hctl = nullptr;    // pinned mirror
   int *dids = nullptr;         // [GL_COUNT][B]
   int *dcounts = nullptr;      // [GL_COUNT]
-  unsigned long long *dcounters = nullptr;  // [0] rounds, [1] Krylov chunks
-  unsigned long long *hcounters = nullptr;
+  GroupLoop *dloop = nullptr;
+  GroupLoop *hloop = nullptr;  // pinned mirror
+  int *hwake = nullptr;        // host-mapped wake flag (a request waits for a free slot)
+  int *dwake = nullptr;        // its device address
   cudaGraphExec_t exec = nullptr;
-  bool nested = false;         // rounds loop on the device (else one round per launch)
-  int round_kernels = 0, chunk_kernels = 0;
+  bool nested = false;         // passes loop on the device (else one pass per launch)
+  bool conditional_service = false;  // the service is a conditional node (else always runs)
+  int pass_kernels = 0, service_kernels = 0;
   long long launches = 0;
   double *stage = nullptr;
   size_t cap_stage = 0;
@@ -290,18 +350,20 @@ struct Group {
       if (allocated[s]) slot_free(slots[s]);
     slots.clear();
     allocated.clear();
-    void *ptrs[] = {dtab, dctl, dids, dcounts, dcounters, stage};
+    void *ptrs[] = {dtab, dctl, dids, dcounts, dloop, stage};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     dtab = nullptr;
     dctl = nullptr;
     dids = dcounts = nullptr;
-    dcounters = nullptr;
+    dloop = nullptr;
     stage = nullptr;
     if (hctl) cudaFreeHost(hctl);
-    if (hcounters) cudaFreeHost(hcounters);
+    if (hloop) cudaFreeHost(hloop);
+    if (hwake) cudaFreeHost(hwake);
     hctl = nullptr;
-    hcounters = nullptr;
+    hloop = nullptr;
+    hwake = dwake = nullptr;
     plan_free(plan);
     if (stream) cudaStreamDestroy(stream);
     if (cap_stream) cudaStreamDestroy(cap_stream);
@@ -330,14 +392,21 @@ struct Group {
     ALLOC(dids, sizeof(int) * GL_COUNT * B);
     ALLOC(dcounts, sizeof(int) * GL_COUNT);
     CK(cudaMemsetAsync(dcounts, 0, sizeof(int) * GL_COUNT, stream));
-    ALLOC(dcounters, sizeof(unsigned long long) * 2);
-    CK(cudaMemsetAsync(dcounters, 0, sizeof(unsigned long long) * 2, stream));
+    ALLOC(dloop, sizeof(GroupLoop));
+    CK(cudaMemsetAsync(dloop, 0, sizeof(GroupLoop), stream));
     CK(cudaMallocHost((void **)&hctl, sizeof(GroupCtl) * B));
     memset(hctl, 0, sizeof(GroupCtl) * B);
-    CK(cudaMallocHost((void **)&hcounters, sizeof(unsigned long long) * 2));
+    CK(cudaMallocHost((void **)&hloop, sizeof(GroupLoop)));
+    memset(hloop, 0, sizeof(GroupLoop));
+    CK(cudaHostAlloc((void **)&hwake, sizeof(int), cudaHostAllocMapped));
+    *(volatile int *)hwake = 0;
+    CK(cudaHostGetDevicePointer((void **)&dwake, hwake, 0));
     CK(cudaStreamSynchronize(stream));
     return 0;
   }
+
+  // Ask a running launch to end at its next pass boundary (any thread).
+  void wake() { __atomic_store_n(hwake, 1, __ATOMIC_RELEASE); }
 
   SlotList list(int l) const {
     SlotList L;
@@ -363,13 +432,12 @@ struct Group {
     return std::max(n, 1);
   }
 
-  // The kernels of a round before the Krylov loop, on stream s (captured into a graph).
-  template <typename T> int issue_round_head(cudaStream_t s, cudaGraphConditionalHandle cond_kry) {
+  // The service of a pass: tail of the finished solves, head of the increment starts,
+  // their constitutive calls, residuals, norms and decisions, and the start of the next
+  // MINRES solves.
+  template <typename T> int issue_service(cudaStream_t s) {
     SlotDev<T> *tab = (SlotDev<T> *)dtab;
     if (voxel) CKR(launch_commit_slip<T>(lctx(GL_COMMIT, s), tab, plan_nslip()));
-    group_begin_kernel<T><<<1, 32, 0, s>>>(tab, dctl, dids, dcounts, B, cond_kry, 1);
-    ++launches;
-    CK(cudaGetLastError());
     if (stress_rates) {
       CKR(launch_tangent_sum<T>(lctx(GL_TSUM, s), tab));
       group_corr_kernel<T><<<1, 32, 0, s>>>(tab, dctl, dids, dcounts, B, plan.V);
@@ -377,90 +445,96 @@ struct Group {
       CK(cudaGetLastError());
     }
     CKR(launch_strain_guess<T>(lctx(GL_FRESH, s), tab));
-    CKR(launch_minres_init<T>(lctx(GL_SOLVE, s), tab));
-    return 0;
-  }
-
-  // The body of the Krylov while node: a chunk of iterations over the active list, then
-  // the list compaction that sets the loop condition.
-  template <typename T> int issue_krylov_chunk(cudaStream_t s, cudaGraphConditionalHandle cond_kry) {
-    SlotDev<T> *tab = (SlotDev<T> *)dtab;
-    for (int i = 0; i < GROUP_KRYLOV_CHUNK; ++i)
-      CKR(launch_krylov_iteration<T>(lctx(GL_KRY, s), tab, voxel));
-    group_minres_continue_kernel<T><<<1, 32, 0, s>>>(tab, dids + GL_KRY * B, dcounts + GL_KRY,
-                                                     cond_kry, dcounters + 1);
-    ++launches;
-    CK(cudaGetLastError());
-    return 0;
-  }
-
-  // The kernels of a round after the Krylov loop.
-  template <typename T>
-  int issue_round_tail(cudaStream_t s, cudaGraphConditionalHandle cond_round, bool use_cond) {
-    SlotDev<T> *tab = (SlotDev<T> *)dtab;
     if (plan.fp64)
-      CKR(launch_update_strain<T>(lctx(GL_SOLVE, s), tab));
+      CKR(launch_update_strain<T>(lctx(GL_TAIL, s), tab));
     else
-      CKR(launch_reproject_update<T>(lctx(GL_SOLVE, s), tab));
+      CKR(launch_reproject_update<T>(lctx(GL_TAIL, s), tab));
     CKR(launch_constitutive<T>(lctx(GL_NEWTON, s), tab, false));
     group_swap_stress_kernel<T><<<1, 32, 0, s>>>(tab, dids, dcounts, B);
     ++launches;
     CKR(launch_residual<T>(lctx(GL_NEWTON, s), tab));
     CKR(launch_norms<T>(lctx(GL_NEWTON, s), tab));
-    group_decide_kernel<T><<<1, 32, 0, s>>>(tab, dctl, dids, dcounts, B, plan.V, cond_round,
-                                            use_cond ? 1 : 0, dcounters);
+    group_decide_kernel<T><<<1, 32, 0, s>>>(tab, dctl, dids, dcounts, B, plan.V, dloop);
     ++launches;
     CK(cudaGetLastError());
+    CKR(launch_minres_init<T>(lctx(GL_ENTER, s), tab));
     return 0;
   }
 
-  // One round (head, Krylov while node, tail) captured into `into` on cap_stream; the
-  // Krylov node's condition handle belongs to `into`.
+  template <typename T> int issue_chunk(cudaStream_t s) {
+    SlotDev<T> *tab = (SlotDev<T> *)dtab;
+    for (int i = 0; i < GROUP_KRYLOV_CHUNK; ++i)
+      CKR(launch_krylov_iteration<T>(lctx(GL_KRY, s), tab, voxel));
+    return 0;
+  }
+
+  // One pass captured into `into` on cap_stream: schedule, the service (a conditional node
+  // when `cond_service`, else unconditional), the Krylov chunk, and the loop condition.
   template <typename T>
-  cudaError_t capture_round(cudaGraph_t into, cudaGraphConditionalHandle cond_round, bool use_cond,
-                            int *rc) {
-    cudaGraphConditionalHandle cond_kry;
-    cudaError_t e = cudaGraphConditionalHandleCreate(&cond_kry, into, 0, 0);
+  cudaError_t capture_pass(cudaGraph_t into, cudaGraphConditionalHandle cond_loop, bool use_loop,
+                           bool cond_service, int *rc) {
+    SlotDev<T> *tab = (SlotDev<T> *)dtab;
+    cudaGraphConditionalHandle cond_srv = 0;
+    cudaError_t e = cudaSuccess;
+    if (cond_service) e = cudaGraphConditionalHandleCreate(&cond_srv, into, 0, 0);
     if (e != cudaSuccess) return e;
     e = cudaStreamBeginCaptureToGraph(cap_stream, into, nullptr, nullptr, 0,
                                       cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
-    *rc = issue_round_head<T>(cap_stream, cond_kry);
-    // the Krylov while node, appended to the capture's current dependencies
-    cudaStreamCaptureStatus cs;
-    const cudaGraphNode_t *deps = nullptr;
-    size_t ndeps = 0;
-    cudaGraph_t capg = nullptr;
-    if (!*rc) e = cudaStreamGetCaptureInfo(cap_stream, &cs, nullptr, &capg, &deps, &ndeps);
-    cudaGraphNodeParams kp = {cudaGraphNodeTypeConditional};
-    kp.conditional.handle = cond_kry;
-    kp.conditional.type = cudaGraphCondTypeWhile;
-    kp.conditional.size = 1;
-    cudaGraphNode_t knode = nullptr;
-    if (!*rc && e == cudaSuccess) e = cudaGraphAddNode(&knode, capg, deps, ndeps, &kp);
-    if (!*rc && e == cudaSuccess)
-      e = cudaStreamUpdateCaptureDependencies(cap_stream, &knode, 1, cudaStreamSetCaptureDependencies);
-    // the Krylov chunk, captured into the node's body on the group's own stream
-    if (!*rc && e == cudaSuccess) {
-      e = cudaStreamBeginCaptureToGraph(stream, kp.conditional.phGraph_out[0], nullptr, nullptr,
-                                        0, cudaStreamCaptureModeThreadLocal);
+    const long long l0 = launches;
+    group_sched_kernel<T><<<1, 32, 0, cap_stream>>>(tab, dctl, dids, dcounts, B, cond_srv,
+                                                     cond_service ? 1 : 0, dloop);
+    ++launches;
+    e = cudaGetLastError();
+    if (e == cudaSuccess && cond_service) {
+      // the service as an IF node appended to the capture's current dependencies, its body
+      // captured on the group's own stream
+      cudaStreamCaptureStatus cs;
+      const cudaGraphNode_t *deps = nullptr;
+      size_t ndeps = 0;
+      cudaGraph_t capg = nullptr;
+      e = cudaStreamGetCaptureInfo(cap_stream, &cs, nullptr, &capg, &deps, &ndeps);
+      cudaGraphNodeParams ip = {cudaGraphNodeTypeConditional};
+      ip.conditional.handle = cond_srv;
+      ip.conditional.type = cudaGraphCondTypeIf;
+      ip.conditional.size = 1;
+      cudaGraphNode_t inode = nullptr;
+      if (e == cudaSuccess) e = cudaGraphAddNode(&inode, capg, deps, ndeps, &ip);
+      if (e == cudaSuccess)
+        e = cudaStreamUpdateCaptureDependencies(cap_stream, &inode, 1, cudaStreamSetCaptureDependencies);
       if (e == cudaSuccess) {
-        const long long lk = launches;
-        *rc = issue_krylov_chunk<T>(stream, cond_kry);
-        chunk_kernels = (int)(launches - lk);
-        cudaGraph_t g2 = nullptr;
-        const cudaError_t e2 = cudaStreamEndCapture(stream, &g2);
-        if (e == cudaSuccess) e = e2;
+        e = cudaStreamBeginCaptureToGraph(stream, ip.conditional.phGraph_out[0], nullptr, nullptr,
+                                          0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+          const long long ls = launches;
+          *rc = issue_service<T>(stream);
+          service_kernels = (int)(launches - ls);
+          cudaGraph_t g2 = nullptr;
+          const cudaError_t e2 = cudaStreamEndCapture(stream, &g2);
+          if (e == cudaSuccess) e = e2;
+        }
       }
+    } else if (e == cudaSuccess) {
+      const long long ls = launches;
+      *rc = issue_service<T>(cap_stream);
+      service_kernels = (int)(launches - ls);
     }
-    if (!*rc && e == cudaSuccess) *rc = issue_round_tail<T>(cap_stream, cond_round, use_cond);
+    if (e == cudaSuccess && !*rc) *rc = issue_chunk<T>(cap_stream);
+    if (e == cudaSuccess && !*rc) {
+      group_loop_kernel<<<1, 32, 0, cap_stream>>>(dctl, B, dloop, dwake, cond_loop,
+                                                  use_loop ? 1 : 0);
+      ++launches;
+      e = cudaGetLastError();
+    }
+    pass_kernels = (int)(launches - l0) - service_kernels;
     cudaGraph_t g1 = nullptr;
     const cudaError_t e1 = cudaStreamEndCapture(cap_stream, &g1);
     return e != cudaSuccess ? e : e1;
   }
 
-  // The rounds loop as nested while nodes (outer: rounds; inner: Krylov chunks), or, when
-  // nesting is not available (SSFFT_NO_DEVICE_LOOP=1 or an error), one round per launch.
+  // The passes loop as a while node holding an IF node (the service), or, when conditional
+  // nodes are not available (SSFFT_NO_DEVICE_LOOP=1 or an error), one pass per launch with
+  // the service always run.
   template <typename T> int build() {
     const char *nl = getenv("SSFFT_NO_DEVICE_LOOP");
     const bool allow_nested = !(nl && nl[0] == '1');
@@ -472,51 +546,33 @@ struct Group {
       cudaError_t e = cudaSuccess;
       int rc = 0;
       if (want_nested) {
-        cudaGraphConditionalHandle cond_round;
-        e = cudaGraphConditionalHandleCreate(&cond_round, graph, 1, cudaGraphCondAssignDefault);
+        cudaGraphConditionalHandle cond_loop;
+        e = cudaGraphConditionalHandleCreate(&cond_loop, graph, 1, cudaGraphCondAssignDefault);
         cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
-        np.conditional.handle = cond_round;
+        np.conditional.handle = cond_loop;
         np.conditional.type = cudaGraphCondTypeWhile;
         np.conditional.size = 1;
         cudaGraphNode_t node;
         if (e == cudaSuccess) e = cudaGraphAddNode(&node, graph, nullptr, 0, &np);
         if (e == cudaSuccess)
-          e = capture_round<T>(np.conditional.phGraph_out[0], cond_round, true, &rc);
+          e = capture_pass<T>(np.conditional.phGraph_out[0], cond_loop, true, true, &rc);
       } else {
-        e = capture_round<T>(graph, 0, false, &rc);
+        e = capture_pass<T>(graph, 0, false, false, &rc);
       }
       if (e == cudaSuccess && !rc) e = cudaGraphInstantiate(&exec, graph, 0);
       cudaGraphDestroy(graph);
       launches = l0;
       if (rc) return rc;
       if (e == cudaSuccess) {
-        round_kernels = 0;  // counted per round from the capture below
         nested = want_nested;
-        return count_round_kernels<T>();
+        conditional_service = want_nested;
+        return 0;
       }
       exec = nullptr;
       cudaGetLastError();
       if (!want_nested)
         return ssfft_internal_fail(SSFFT_E_CUDA, std::string("group graph: ") + cudaGetErrorString(e));
     }
-    return 0;
-  }
-
-  // Kernels of one round outside the Krylov loop (for the launch count): the head and the
-  // tail issue a fixed number of kernels.
-  template <typename T> int count_round_kernels() {
-    int n = 0;
-    if (voxel) n += 1;                 // commit of the slip resistances
-    n += 1;                            // begin
-    if (stress_rates) n += 2;          // tangent sum, correction
-    n += 2;                            // strain guess, MINRES init
-    const bool plane = three_pass<double>(plan);
-    n += plane ? 3 : 5;                // reprojection (mixed) or update (FP64: 1)
-    if (plan.fp64) n -= (plane ? 3 : 5) - 1;
-    n += 1 + 1;                        // constitutive, stress swap
-    n += plane ? 3 : 5;                // residual
-    n += 1 + 1;                        // norms, decide
-    round_kernels = n;
     return 0;
   }
 
@@ -583,34 +639,36 @@ struct Group {
     return 0;
   }
 
-  // Advance the live slots until one finishes (or the round cap).  The control blocks
-  // come back to hctl.
+  // Advance the live slots until one finishes, the host raises the wake flag, or the pass
+  // cap.  The control blocks come back to hctl.
   int run() {
     CK(cudaSetDevice(device));
     if (!exec) {
       const int rc = plan.fp64 ? build<double>() : build<float>();
       if (rc) return rc;
     }
-    CK(cudaMemcpyAsync(hcounters, dcounters, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                       stream));
+    CK(cudaMemcpyAsync(hloop, dloop, sizeof(GroupLoop), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
-    const unsigned long long r0 = hcounters[0], k0 = hcounters[1];
+    const unsigned long long p0 = hloop->passes, s0 = hloop->services;
+    hloop->finished = 0;
+    hloop->launch_passes = 0;
+    CK(cudaMemcpyAsync(dloop, hloop, sizeof(GroupLoop), cudaMemcpyHostToDevice, stream));
     for (;;) {
       CK(cudaGraphLaunch(exec, stream));
       CK(cudaMemcpyAsync(hctl, dctl, sizeof(GroupCtl) * B, cudaMemcpyDeviceToHost, stream));
-      CK(cudaMemcpyAsync(hcounters, dcounters, 2 * sizeof(unsigned long long),
-                         cudaMemcpyDeviceToHost, stream));
+      CK(cudaMemcpyAsync(hloop, dloop, sizeof(GroupLoop), cudaMemcpyDeviceToHost, stream));
       CK(cudaStreamSynchronize(stream));
       if (nested) break;
-      int live = 0, done = 0;
-      for (int s = 0; s < B; ++s) {
+      int live = 0;
+      for (int s = 0; s < B; ++s)
         if (hctl[s].state == GS_FRESH || hctl[s].state == GS_SOLVE) ++live;
-        if (hctl[s].state == GS_DONE || hctl[s].state == GS_FAILED) ++done;
-      }
-      if (live == 0 || done > 0) break;
+      if (live == 0 || hloop->finished > 0 || __atomic_load_n(hwake, __ATOMIC_ACQUIRE) ||
+          hloop->launch_passes >= GROUP_PASS_CAP)
+        break;
     }
-    const unsigned long long rounds = hcounters[0] - r0, chunks = hcounters[1] - k0;
-    launches += (long long)rounds * round_kernels + (long long)chunks * chunk_kernels;
+    const unsigned long long passes = hloop->passes - p0, services = hloop->services - s0;
+    launches += (long long)passes * pass_kernels +
+                (long long)(conditional_service ? services : passes) * service_kernels;
     return 0;
   }
 
@@ -678,3 +736,9 @@ __attribute__((visibility("hidden"))) int group_release_slot(Group *g, int s) {
   return g->set_state(s, GS_EMPTY);
 }
 __attribute__((visibility("hidden"))) long long group_launches(Group *g) { return g->launches; }
+__attribute__((visibility("hidden"))) void group_wake(Group *g) {
+  if (g && g->hwake) g->wake();
+}
+__attribute__((visibility("hidden"))) void group_clear_wake(Group *g) {
+  if (g && g->hwake) __atomic_store_n(g->hwake, 0, __ATOMIC_RELEASE);
+}

@@ -32,3 +32,7 @@ void group_slot_result(Group *g, int s, ssfft_solve_out *o);
 int group_read_stress(Group *g, int s, double *dst);
 int group_release_slot(Group *g, int s);
 long long group_launches(Group *g);
+// Ask the group's running launch to return at its next pass boundary (any thread), and
+// clear that request (the group's driver thread, before it runs the group again).
+void group_wake(Group *g);
+void group_clear_wake(Group *g);

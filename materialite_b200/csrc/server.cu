@@ -6,9 +6,11 @@
 // advance together, every kernel launch covering all of them.  A group's driver thread
 // loads queued requests into free slots (a slot's device memory is allocated on its first
 // use, when it fits both the server's budget and cudaMemGetInfo's free memory), runs the
-// group's rounds graph until some request finishes, returns the finished requests'
-// results, and refills.  Requests that arrive while others run join at the next round
-// boundary of their class; classes run concurrently on their own streams.
+// group's graph until some request finishes, returns the finished requests' results, and
+// refills.  A request that arrives while its class runs with a free slot raises the
+// group's wake flag, and the running graph returns at its next pass boundary (a few Krylov
+// iterations) so that the request is loaded and joins the others; classes run
+// concurrently on their own streams.
 //
 // A request's arithmetic does not depend on what else runs: every reduction of a slot is
 // private to it and summed in a fixed order, so a result is bitwise the same alone and in
@@ -94,6 +96,8 @@ struct GroupRunner {
   ClassInfo info;
   ssfft_config proto;
   Group *g = nullptr;
+  std::atomic<Group *> gpub{nullptr};  // g once initialised, for the submitting threads
+  int n_resident = 0;                  // occupied slots (guarded by srv->mu)
   bool init_failed = false;
   std::string init_message;
   std::deque<GroupJob *> queue;     // guarded by srv->mu
@@ -145,6 +149,7 @@ struct GroupRunner {
       }
       queue.pop_front();
       resident[s] = j;
+      ++n_resident;
       start[s] = srv->now();
       loaded.push_back(s);
     }
@@ -179,6 +184,7 @@ struct GroupRunner {
     resident.assign(srv->max_slots, nullptr);
     start.assign(srv->max_slots, 0.0);
     counted.assign(srv->max_slots, false);
+    if (!init_failed) gpub.store(g);
     for (;;) {
       std::vector<int> loaded;
       {
@@ -194,6 +200,8 @@ struct GroupRunner {
           } else {
             reject_unfit();
             admit(loaded);
+            // submissions from here on find the slots as they are now
+            if (g) group_clear_wake(g);
           }
           bool any = false;
           for (GroupJob *j : resident) any = any || j;
@@ -212,6 +220,8 @@ struct GroupRunner {
           delete resident[s];
           resident[s] = nullptr;
           group_release_slot(g, s);
+          std::lock_guard<std::mutex> lk(srv->mu);
+          --n_resident;
         }
       }
       bool any = false;
@@ -246,6 +256,10 @@ struct GroupRunner {
         group_release_slot(g, s);
         delete j;
         resident[s] = nullptr;
+        {
+          std::lock_guard<std::mutex> lk(srv->mu);
+          --n_resident;
+        }
         srv->post(c);
       }
     }
@@ -311,8 +325,12 @@ extern "C" int ssfft_server_submit(ssfft_server *s, const ssfft_request *req) {
     rp->th = std::thread(&GroupRunner::run, rp);
   }
   j->submit_time = s->now();
-  it->second->queue.push_back(j);
+  GroupRunner *r = it->second.get();
+  r->queue.push_back(j);
   ++s->outstanding;
+  // a free slot: the running graph of the class returns at its next pass to take it
+  Group *g = r->gpub.load();
+  if (g && r->n_resident < s->max_slots) group_wake(g);
   s->cv.notify_all();
   return 0;
 }

@@ -895,9 +895,12 @@ extern "C" int ssfft_timer(ssfft_handle *h, int start, double *seconds) {
 
 template <typename T> static int profile_impl(ssfft_handle *h, int reps, double *sec) {
   SlotDev<T> &m = mirror<T>(h->sb);
+  const SlotDev<T> saved = m;
   const LaunchCtx c = ctx(h);
-  // a live MINRES state on the residual of the current stress (never marked done); call
-  // after a solve so that the stress field is not uniform
+  // a live MINRES state on the residual of the committed stress (never marked done); call
+  // after a solve so that the stress field is not uniform.  After a commit the latest-stress
+  // buffer holds the previous increment's field, so the committed one stands in for it.
+  m.sig = m.sig_old;
   for (int k = 0; k < 6; ++k) m.sbar[k] = 0.0;
   m.rtol = 0.0;
   m.maxiter = (long long)1 << 60;
@@ -922,6 +925,14 @@ template <typename T> static int profile_impl(ssfft_handle *h, int reps, double 
   }
   for (int i = 0; i < 8; ++i) sec[i] = acc[i] / reps;
   sec[6] = 0.0;
+  // every timed iteration must have done its work: a state that stopped (a zero or
+  // exactly solved residual) would time kernels that skip their items
+  CK(cudaMemcpyAsync(h->h_st, h->sb.st, sizeof(MinresState), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const bool live = !h->h_st->done && h->h_st->itn == reps;
+  m = saved;
+  CKR(upload(h));
+  if (!live) return fail(SSFFT_E_INVALID, "profiled Krylov state stopped early: timings void");
   return 0;
 }
 

@@ -246,6 +246,9 @@ class SolveStats:
     newton_iterations: list = field(default_factory=list)
     krylov_iterations: list = field(default_factory=list)
     device_seconds: float = 0.0
+    # one record per attempted increment: time, dt, converged, Newton and Krylov
+    # iterations, final equilibrium error, most constitutive iterations
+    attempts: list = field(default_factory=list)
 
 
 # the reference's logger name (small_strain_fft.py:53)
@@ -293,6 +296,9 @@ def solve(handle, dstrain, dstress, stress, end_time=1.0, initial_time_increment
             stats.newton_iterations.append(out.newton_iterations)
             stats.krylov_iterations.append(out.krylov_iterations)
             stats.device_seconds += handle.stats()[0]
+            stats.attempts.append((t, dt, bool(out.converged), int(out.newton_iterations),
+                                   int(out.krylov_iterations), float(out.equilibrium_error),
+                                   int(out.max_constitutive_iterations)))
         if out.converged:
             handle.commit(1.0)
             summed_vm += out.mean_von_mises_stress

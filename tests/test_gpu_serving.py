@@ -98,7 +98,7 @@ def evp_requests(seeds, steps=(3, 5)):
 
 def test_batched_requests_identical_alone_and_in_the_group():
     """Four crystal-plasticity requests of one class share a group: every kernel launch
-    covers all four, their Newton iterations advance in common rounds, and each result is
+    covers all four (each at its own Newton iteration), and each result is
     still bitwise the one it gets alone (every reduction is private to its slot)."""
     seeds = [31, 32, 33, 34]
     alone = []
@@ -142,3 +142,28 @@ def test_group_time_loop_matches_python_loop_crystal_plasticity():
                    end_time=r.dt * r.steps, initial_time_increment=r.dt)
     h.close()
     assert np.array_equal(out["stress"], r.stress)
+
+
+def test_late_request_joins_a_running_group():
+    """A request that arrives while a long request of its class is running takes a free
+    slot at once (the running graph returns at its next pass boundary to load it) instead of
+    waiting for the long request to finish, and its result is still bitwise the one it gets
+    alone."""
+    long_r, short_r = evp_requests([51, 52], steps=(4, 4))
+    long_r.steps = 60
+    short_r.steps = 2
+    short_r.arrival = 0.05
+    alone = evp_requests([52], steps=(4, 4))[0]
+    alone.steps = 2
+    srv = RVEServer(max_slots=1)
+    comps, _ = run_stream(srv, [alone])
+    srv.close()
+    assert comps[0].status == 0
+    srv = RVEServer(max_slots=4)
+    comps, _ = run_stream(srv, [long_r, short_r])
+    srv.close()
+    a, b = comps
+    assert a.status == 0 and b.status == 0
+    assert b.submit_time > a.start_time          # the long request was running
+    assert b.end_time < a.end_time               # and the short one did not wait for it
+    assert np.array_equal(short_r.stress, alone.stress)
