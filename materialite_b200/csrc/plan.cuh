@@ -125,12 +125,12 @@ static int resident_clusters(void (*f)(A...), int C, int threads, size_t smem, i
   return n;
 }
 
-// Persistent launch of a cluster kernel: as many clusters as are resident at once, but no
-// more than there are items.
+// Persistent launch of a cluster kernel of `threads` threads a block: as many clusters as
+// are resident at once, but no more than there are items.
 template <typename... P, typename... A>
-static int launch_clustered(void (*f)(P...), int C, size_t smem, long long items, int dev,
-                            cudaStream_t stream, A &&...args) {
-  const int ncl = (int)std::max(1LL, std::min<long long>(items, resident_clusters(f, C, CLUSTER_THREADS, smem, dev)));
+static int launch_clustered(void (*f)(P...), int C, int threads, size_t smem, long long items,
+                            int dev, cudaStream_t stream, A &&...args) {
+  const int ncl = (int)std::max(1LL, std::min<long long>(items, resident_clusters(f, C, threads, smem, dev)));
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -138,7 +138,7 @@ static int launch_clustered(void (*f)(P...), int C, size_t smem, long long items
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
   cfg.gridDim = dim3((unsigned)(ncl * C));
-  cfg.blockDim = dim3(CLUSTER_THREADS);
+  cfg.blockDim = dim3(threads);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = stream;
   cfg.attrs = at;
@@ -234,12 +234,17 @@ template <typename T> static bool plane_ok(const GridPlan &p) {
 
 // Blocks per cluster of the cluster plane passes (0: not used): the smallest C in 2, 4, 8
 // whose blocks fit the shared-memory budget, for grids whose plane does not fit one block.
-// SSFFT_CLUSTER=C asks for a larger C where it divides the plane.
+// SSFFT_CLUSTER=C asks for clusters of at least C blocks, also where one block would do.
+static int env_int(const char *name) {
+  const char *v = getenv(name);
+  return v ? atoi(v) : 0;
+}
+
 template <typename T> static int cluster_size(const GridPlan &p) {
-  if (!p.use_plane || plane_ok<T>(p)) return 0;
+  if (!p.use_plane) return 0;
+  const int want = env_int("SSFFT_CLUSTER");
+  if (want <= 0 && plane_ok<T>(p)) return 0;
   const int hs = (p.nz % 2 == 0) ? p.nz / 2 : p.hz;
-  const char *env = getenv("SSFFT_CLUSTER");
-  const int want = env ? atoi(env) : 0;
   for (int C = 2; C <= CLUSTER_MAX; C *= 2) {
     if (p.ny % C != 0 || (2 * hs) % C != 0 || C < want) continue;
     if (smem_cplane_bytes<T>(p.ny, p.nz, hs, C) <= PLANE_SMEM_LIMIT) return C;
@@ -257,6 +262,17 @@ template <typename T> static ClusterGeo cluster_geo(const GridPlan &p, int C) {
   q.fd_R = make_fastdiv((uint32_t)q.R);
   q.fd_Lq = make_fastdiv((uint32_t)q.Lq);
   return q;
+}
+
+// Threads of a cluster block: 512 when two blocks fit an SM's shared memory, else 1024
+// (SSFFT_CLUSTER_THREADS=512 or 1024 overrides where the memory allows).
+template <typename T> static int cluster_threads(const GridPlan &p, int C) {
+  const int hs = (p.nz % 2 == 0) ? p.nz / 2 : p.hz;
+  const bool two = smem_cplane_bytes<T>(p.ny, p.nz, hs, C) <= 113 * 1024;
+  const int want = env_int("SSFFT_CLUSTER_THREADS");
+  if (want == 1024) return 1024;
+  if (want == 512) return 512;
+  return two ? 512 : 1024;
 }
 
 // The projection runs as three passes (z and y fused, in one block or one cluster).
@@ -329,8 +345,7 @@ static int plan_create(GridPlan &p, const ssfft_config *cfg, cudaStream_t stream
   make_axis_plan(p.nx, p.px);
   make_axis_plan(p.ny, p.py);
   make_axis_plan(p.nz, p.pz);
-  const char *np = getenv("SSFFT_NO_PLANE");
-  p.use_plane = !(np && np[0] == '1');
+  p.use_plane = env_int("SSFFT_NO_PLANE") != 1;
   CKR(plan_tiles(p));
   // FFT tables: float ones for the mixed-mode Krylov transforms, double ones for every
   // double-precision transform
@@ -398,17 +413,17 @@ template <typename T, typename TF, int PT> static int plane_attrs(int m) {
   return 0;
 }
 
-template <typename T, typename TF> static int cluster_attrs(int m) {
-  CKR(smem_attr(zyfwd_cl_kernel<T, TF, PRO_INPUT>, m));
-  CKR(smem_attr(zyfwd_cl_kernel<T, TF, PRO_RESIDUAL>, m));
-  CKR(smem_attr(zyfwd_cl_kernel<T, TF, PRO_REPROJECT>, m));
-  CKR(smem_attr(yzinv_cl_kernel<T, TF, EPI_STORE>, m));
-  CKR(smem_attr(yzinv_cl_kernel<T, TF, EPI_RESIDUAL>, m));
-  CKR(smem_attr(yzinv_cl_kernel<T, TF, EPI_REPROJECT>, m));
+template <typename T, typename TF, int PT> static int cluster_attrs(int m) {
+  CKR(smem_attr(zyfwd_cl_kernel<T, TF, PRO_INPUT, PT>, m));
+  CKR(smem_attr(zyfwd_cl_kernel<T, TF, PRO_RESIDUAL, PT>, m));
+  CKR(smem_attr(zyfwd_cl_kernel<T, TF, PRO_REPROJECT, PT>, m));
+  CKR(smem_attr(yzinv_cl_kernel<T, TF, EPI_STORE, PT>, m));
+  CKR(smem_attr(yzinv_cl_kernel<T, TF, EPI_RESIDUAL, PT>, m));
+  CKR(smem_attr(yzinv_cl_kernel<T, TF, EPI_REPROJECT, PT>, m));
   if (sizeof(T) == sizeof(TF)) {
-    CKR(smem_attr(zyfwd_cl_kernel<T, T, PRO_TANGENT_TABLE>, m));
-    CKR(smem_attr(zyfwd_cl_kernel<T, T, PRO_TANGENT_VOXEL>, m));
-    CKR(smem_attr(yzinv_cl_kernel<T, T, EPI_MINRES>, m));
+    CKR(smem_attr(zyfwd_cl_kernel<T, T, PRO_TANGENT_TABLE, PT>, m));
+    CKR(smem_attr(zyfwd_cl_kernel<T, T, PRO_TANGENT_VOXEL, PT>, m));
+    CKR(smem_attr(yzinv_cl_kernel<T, T, EPI_MINRES, PT>, m));
   }
   return 0;
 }
@@ -430,7 +445,8 @@ template <typename T, typename TF> static int set_kernel_attrs(size_t smax) {
   CKR(smem_attr(zinv_kernel<T, TF, EPI_REPROJECT>, m));
   CKR((plane_attrs<T, TF, 512>(m)));
   CKR((plane_attrs<T, TF, 1024>(m)));
-  CKR((cluster_attrs<T, TF>(m)));
+  CKR((cluster_attrs<T, TF, 512>(m)));
+  CKR((cluster_attrs<T, TF, 1024>(m)));
   if (sizeof(T) == sizeof(TF)) {
     CKR(smem_attr(constitutive_kernel<T>, (int)constitutive_smem_bytes()));
     CKR(smem_attr(zfwd_kernel<T, T, PRO_TANGENT_TABLE>, m));
@@ -847,7 +863,11 @@ static int launch_projector(const LaunchCtx &c, const SlotDev<TF> *tab, ExtIO<TF
     const ClusterGeo q = cluster_geo<T>(p, C);
     const size_t sp = smem_cplane_bytes<T>(p.ny, p.nz, g.hs, C);
     const long long it = (long long)c.cap * items_plane(g);
-    CKR(launch_clustered(zyfwd_cl_kernel<T, TF, PRO>, C, sp, it, dev, c.stream, g, q, tab, c.list, io));
+    const int pt = cluster_threads<T>(p, C);
+    if (pt == 1024)
+      CKR(launch_clustered(zyfwd_cl_kernel<T, TF, PRO, 1024>, C, 1024, sp, it, dev, c.stream, g, q, tab, c.list, io));
+    else
+      CKR(launch_clustered(zyfwd_cl_kernel<T, TF, PRO, 512>, C, 512, sp, it, dev, c.stream, g, q, tab, c.list, io));
     rec(1);
     rec(2);
     auto kx = xpass_kernel<T, TF, KRY>;
@@ -855,7 +875,10 @@ static int launch_projector(const LaunchCtx &c, const SlotDev<TF> *tab, ExtIO<TF
          sx, c.stream>>>(g, tab, c.list);
     rec(3);
     rec(4);
-    CKR(launch_clustered(yzinv_cl_kernel<T, TF, EPI>, C, sp, it, dev, c.stream, g, q, tab, c.list, io));
+    if (pt == 1024)
+      CKR(launch_clustered(yzinv_cl_kernel<T, TF, EPI, 1024>, C, 1024, sp, it, dev, c.stream, g, q, tab, c.list, io));
+    else
+      CKR(launch_clustered(yzinv_cl_kernel<T, TF, EPI, 512>, C, 512, sp, it, dev, c.stream, g, q, tab, c.list, io));
     rec(5);
     if (c.launches) *c.launches += 3;
   } else {

@@ -1021,10 +1021,10 @@ template <typename T> inline size_t smem_cplane_bytes(int ny, int nz, int hs, in
   return (2 * (size_t)cplane_buf_elems(ny, nz, hs, C) + ny + nz) * sizeof(cplx<T>);
 }
 
-#define CLUSTER_THREADS 1024
-
-template <typename T, typename TF, int PRO>
-__global__ void __launch_bounds__(CLUSTER_THREADS, 1)
+// Blocks of PT = 1024 threads (one per SM) or 512 (two per SM when their shared memory
+// fits, so that one block's loads overlap the other's transforms), at most 64 registers.
+template <typename T, typename TF, int PRO, int PT>
+__global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     zyfwd_cl_kernel(Grid<T> g, ClusterGeo cq, const SlotDev<TF> *__restrict__ tab,
                     SlotList list, ExtIO<TF> io) {
   namespace cg = cooperative_groups;
@@ -1103,8 +1103,8 @@ __global__ void __launch_bounds__(CLUSTER_THREADS, 1)
   }
 }
 
-template <typename T, typename TF, int EPI>
-__global__ void __launch_bounds__(CLUSTER_THREADS, 1)
+template <typename T, typename TF, int EPI, int PT>
+__global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     yzinv_cl_kernel(Grid<T> g, ClusterGeo cq, const SlotDev<TF> *__restrict__ tab,
                     SlotList list, ExtIO<TF> io) {
   namespace cg = cooperative_groups;

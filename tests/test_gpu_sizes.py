@@ -67,6 +67,15 @@ def use_path(monkeypatch, path):
         monkeypatch.delenv("SSFFT_NO_PLANE", raising=False)
 
 
+def use_cluster(monkeypatch, path):
+    """plane: the default plane-fused path (clusters where one block cannot hold the
+    plane); clusterN: clusters of at least N blocks; five_pass: no plane fusion."""
+    monkeypatch.delenv("SSFFT_CLUSTER", raising=False)
+    use_path(monkeypatch, "five_pass" if path == "five_pass" else "plane")
+    if path.startswith("cluster"):
+        monkeypatch.setenv("SSFFT_CLUSTER", path[len("cluster"):])
+
+
 @functools.lru_cache(maxsize=None)
 def elastic_reference(dims, steps, grains=40, seed=3):
     R = micro(dims, grains, seed)
@@ -117,11 +126,12 @@ def run_evp(dims, R, steps, precision):
     return out
 
 
-@pytest.mark.parametrize("path", ["plane", "five_pass"])
+@pytest.mark.parametrize("path", ["plane", "cluster2", "five_pass"])
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-5)])
 def test_elastic_48(precision, tol, path, monkeypatch):
-    """48^3 (radix 3 x 16), 40 periodic Voronoi grains, two load steps."""
-    use_path(monkeypatch, path)
+    """48^3 (radix 3 x 16), 40 periodic Voronoi grains, two load steps; cluster2 runs the
+    plane passes on 2-block clusters although one block would hold the plane."""
+    use_cluster(monkeypatch, path)
     dims = (48, 48, 48)
     R, ref, ost = elastic_reference(dims, 2)
     out, st = run_elastic(dims, R, 2, precision)
@@ -143,15 +153,6 @@ def test_elastic_96(precision, tol):
     assert rel_l2(out["strain"], ref["strain"]) < tol
     if precision == "fp64":
         assert_counts_close(st, ost)
-
-
-def use_cluster(monkeypatch, path):
-    """plane: the default plane-fused path (clusters where one block cannot hold the
-    plane); clusterN: clusters of at least N blocks; five_pass: no plane fusion."""
-    monkeypatch.delenv("SSFFT_CLUSTER", raising=False)
-    use_path(monkeypatch, "five_pass" if path == "five_pass" else "plane")
-    if path.startswith("cluster"):
-        monkeypatch.setenv("SSFFT_CLUSTER", path[len("cluster"):])
 
 
 @pytest.mark.parametrize("path", ["plane", "cluster8", "five_pass"])
@@ -202,12 +203,13 @@ def test_evp_cluster(precision, tol, path, monkeypatch):
     assert rel_l2(out["strain"], ref["strain"]) < tol
 
 
-@pytest.mark.parametrize("path", ["plane", "five_pass"])
+@pytest.mark.parametrize("path", ["plane", "cluster4", "five_pass"])
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-6), ("mixed", 1e-5)])
 def test_evp_32(precision, tol, path, monkeypatch):
     """Serving-size crystal plasticity: 32^3, 40 grains, FCC Voce (config-3 parameters at
-    latent ratio 1), two load steps of dt 0.6 past the onset of slip."""
-    use_path(monkeypatch, path)
+    latent ratio 1), two load steps of dt 0.6 past the onset of slip; cluster4 on 4-block
+    clusters of 512 threads."""
+    use_cluster(monkeypatch, path)
     dims = (32, 32, 32)
     R, ref = evp_reference(dims, 2)
     out = run_evp(dims, R, 2, precision)
