@@ -232,9 +232,11 @@ template <typename T> static bool plane_ok(const GridPlan &p) {
   return p.use_plane && smem_plane_bytes<T>(p.ny, p.nz) <= PLANE_SMEM_LIMIT;
 }
 
-// Blocks per cluster of the cluster plane passes (0: not used): the smallest C in 2, 4, 8
-// whose blocks fit the shared-memory budget, for grids whose plane does not fit one block.
-// SSFFT_CLUSTER=C asks for clusters of at least C blocks, also where one block would do.
+// Blocks per cluster of the cluster plane passes (0: not used), for grids whose plane does
+// not fit one block: the smallest C in 2, 4, 8 whose blocks fit two to an SM, else the
+// smallest whose blocks fit at all (a single block per SM leaves its loads and its
+// transforms without overlap).  SSFFT_CLUSTER=C asks for clusters of at least C blocks,
+// also where one block would hold the plane.
 static int env_int(const char *name) {
   const char *v = getenv(name);
   return v ? atoi(v) : 0;
@@ -245,10 +247,16 @@ template <typename T> static int cluster_size(const GridPlan &p) {
   const int want = env_int("SSFFT_CLUSTER");
   if (want <= 0 && plane_ok<T>(p)) return 0;
   const int hs = (p.nz % 2 == 0) ? p.nz / 2 : p.hz;
-  for (int C = 2; C <= CLUSTER_MAX; C *= 2) {
-    if (p.ny % C != 0 || (2 * hs) % C != 0 || C < want) continue;
-    if (smem_cplane_bytes<T>(p.ny, p.nz, hs, C) <= PLANE_SMEM_LIMIT) return C;
-  }
+  auto fits = [&](int C, size_t lim) {
+    return p.ny % C == 0 && (2 * hs) % C == 0 && C >= want &&
+           smem_cplane_bytes<T>(p.ny, p.nz, hs, C) <= lim;
+  };
+  // the smallest cluster whose blocks fit two to an SM (512 threads each), else the
+  // smallest whose blocks fit at all
+  for (int C = 2; C <= CLUSTER_MAX; C *= 2)
+    if (fits(C, 113 * 1024)) return C;
+  for (int C = 2; C <= CLUSTER_MAX; C *= 2)
+    if (fits(C, PLANE_SMEM_LIMIT)) return C;
   return 0;
 }
 
@@ -833,7 +841,29 @@ static int launch_projector(const LaunchCtx &c, const SlotDev<TF> *tab, ExtIO<TF
   const size_t sx = smem_x_bytes<T>(p.kx, p.nx);
   const int dev = p.dev;
   rec(0);
-  if (plane_ok<T>(p)) {
+  if (const int C = cluster_size<T>(p)) {
+    const ClusterGeo q = cluster_geo<T>(p, C);
+    const size_t sp = smem_cplane_bytes<T>(p.ny, p.nz, g.hs, C);
+    const long long it = (long long)c.cap * items_plane(g);
+    const int pt = cluster_threads<T>(p, C);
+    if (pt == 1024)
+      CKR(launch_clustered(zyfwd_cl_kernel<T, TF, PRO, 1024>, C, 1024, sp, it, dev, c.stream, g, q, tab, c.list, io));
+    else
+      CKR(launch_clustered(zyfwd_cl_kernel<T, TF, PRO, 512>, C, 512, sp, it, dev, c.stream, g, q, tab, c.list, io));
+    rec(1);
+    rec(2);
+    auto kx = xpass_kernel<T, TF, KRY>;
+    kx<<<persistent_grid(kx, XPASS_THREADS, sx, (long long)c.cap * items_x(g), dev), XPASS_THREADS,
+         sx, c.stream>>>(g, tab, c.list);
+    rec(3);
+    rec(4);
+    if (pt == 1024)
+      CKR(launch_clustered(yzinv_cl_kernel<T, TF, EPI, 1024>, C, 1024, sp, it, dev, c.stream, g, q, tab, c.list, io));
+    else
+      CKR(launch_clustered(yzinv_cl_kernel<T, TF, EPI, 512>, C, 512, sp, it, dev, c.stream, g, q, tab, c.list, io));
+    rec(5);
+    if (c.launches) *c.launches += 3;
+  } else if (plane_ok<T>(p)) {
     const size_t sp = smem_plane_bytes<T>(p.ny, p.nz);
     const long long it = (long long)c.cap * items_plane(g);
     if (plane_threads<T>(p) == 1024) {
@@ -857,28 +887,6 @@ static int launch_projector(const LaunchCtx &c, const SlotDev<TF> *tab, ExtIO<TF
       auto ki = yzinv_kernel<T, TF, EPI, 512>;
       ki<<<persistent_grid(ki, 512, sp, it, dev), 512, sp, c.stream>>>(g, tab, c.list, io);
     }
-    rec(5);
-    if (c.launches) *c.launches += 3;
-  } else if (const int C = cluster_size<T>(p)) {
-    const ClusterGeo q = cluster_geo<T>(p, C);
-    const size_t sp = smem_cplane_bytes<T>(p.ny, p.nz, g.hs, C);
-    const long long it = (long long)c.cap * items_plane(g);
-    const int pt = cluster_threads<T>(p, C);
-    if (pt == 1024)
-      CKR(launch_clustered(zyfwd_cl_kernel<T, TF, PRO, 1024>, C, 1024, sp, it, dev, c.stream, g, q, tab, c.list, io));
-    else
-      CKR(launch_clustered(zyfwd_cl_kernel<T, TF, PRO, 512>, C, 512, sp, it, dev, c.stream, g, q, tab, c.list, io));
-    rec(1);
-    rec(2);
-    auto kx = xpass_kernel<T, TF, KRY>;
-    kx<<<persistent_grid(kx, XPASS_THREADS, sx, (long long)c.cap * items_x(g), dev), XPASS_THREADS,
-         sx, c.stream>>>(g, tab, c.list);
-    rec(3);
-    rec(4);
-    if (pt == 1024)
-      CKR(launch_clustered(yzinv_cl_kernel<T, TF, EPI, 1024>, C, 1024, sp, it, dev, c.stream, g, q, tab, c.list, io));
-    else
-      CKR(launch_clustered(yzinv_cl_kernel<T, TF, EPI, 512>, C, 512, sp, it, dev, c.stream, g, q, tab, c.list, io));
     rec(5);
     if (c.launches) *c.launches += 3;
   } else {

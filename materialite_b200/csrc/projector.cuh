@@ -131,6 +131,11 @@ struct MinresState {
   int istop, done;
 };
 
+// A slot's "solve done" flag, read by every thread from L2.  Within a launch the flag of a
+// slot is written only by the slot's last item to arrive, after every item of the slot has
+// read it, so all threads of a block read the same value and no barrier is needed.
+__device__ __forceinline__ bool slot_done(const MinresState *st) { return __ldcg(&st->done) != 0; }
+
 // Caller-owned input and output of the plain projection (PRO_INPUT / EPI_STORE).
 template <typename TF> struct ExtIO {
   const TF *in;
@@ -385,7 +390,7 @@ __device__ __forceinline__ void load_table(cplx<T> *dst, const cplx<T> *src, int
 
 // Block-uniform "skip this item": a Krylov item of a slot whose solve is done.
 template <typename TF, int PRO> __device__ __forceinline__ bool skip_item(const SlotDev<TF> &S) {
-  if constexpr (PRO_IS_KRYLOV(PRO)) return block_read_flag(&S.st->done) != 0;
+  if constexpr (PRO_IS_KRYLOV(PRO)) return slot_done(S.st);
   return false;
 }
 
@@ -481,10 +486,11 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
   load_table<T>(tw, g.twz, nz);
   const int per = items_z(g);
   const int n_items = list_items(list, per);
+  int staged = -1;  // slot whose descriptor sdesc holds
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int k = udiv(item, g.fd_it_z);
     const int local = item - k * per;
-    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc);
+    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc, staged);
     if (skip_item<TF, PRO>(S)) continue;
     const long long line0 = (long long)local * g.lz;
     const int nl = (int)min((long long)g.lz, nlines_all - line0);
@@ -526,7 +532,6 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
     if constexpr (PRO_IS_KRYLOV(PRO)) {
       if (u.on) finish_pending_update(S, xx, local, per, red);
     }
-    __syncthreads();
   }
 }
 
@@ -547,7 +552,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     const int k = udiv(item, g.fd_it_y);
     const int local = item - k * per;
     const SlotDev<TF> &S = tab[list.ids[k]];
-    if (KRY && block_read_flag(&S.st->done)) continue;
+    if (KRY && slot_done(S.st)) continue;
     const int c = udiv(local, g.fd_nkynx);
     const int r1 = local - c * g.nky * g.nx;
     const int x = udiv(r1, g.fd_nky);
@@ -568,7 +573,6 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
       const int y = udiv(e, g.fd_ky[ti]), kk = e - y * nk;
       base[(long long)y * hs + kk] = res[y * nk + kk];
     }
-    __syncthreads();
   }
 }
 
@@ -635,7 +639,7 @@ __global__ void __launch_bounds__(XPASS_THREADS)
     const int kk_slot = udiv(item, g.fd_it_x);
     const int local = item - kk_slot * per;
     const SlotDev<TF> &S = tab[list.ids[kk_slot]];
-    if (KRY && block_read_flag(&S.st->done)) continue;
+    if (KRY && slot_done(S.st)) continue;
     const int y = udiv(local, g.fd_nkx);
     const int kb = local - y * g.nkx;
     const int k0 = kb * g.kx;
@@ -669,7 +673,6 @@ __global__ void __launch_bounds__(XPASS_THREADS)
       const int x = udiv(rem, g.fd_kx[ti]), kk = rem - x * nk;
       spec[c * g.S + ((long long)x * ny + y) * hs + k0 + kk] = out[c * sst + x * nk + kk];
     }
-    __syncthreads();
   }
 }
 
@@ -691,11 +694,12 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
   load_table<T>(tw, g.twz, nz);
   const int per = items_z(g);
   const int n_items = list_items(list, per);
+  int staged = -1;  // slot whose descriptor sdesc holds
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int k = udiv(item, g.fd_it_z);
     const int local = item - k * per;
-    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc);
-    if (EPI == EPI_MINRES && block_read_flag(&S.st->done)) continue;
+    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc, staged);
+    if (EPI == EPI_MINRES && slot_done(S.st)) continue;
     const long long line0 = (long long)local * g.lz;
     const int nl = (int)min((long long)g.lz, nlines_all - line0);
     const int ti = (nl == g.lz) ? 0 : 1;
@@ -778,7 +782,6 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
       }
     }
     finish_inverse<TF, EPI>(S, acc0, acc1, acc2, local, per, red);
-    __syncthreads();
   }
 }
 
@@ -896,10 +899,11 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
   const int per = items_plane(g);
   const int n_items = list_items(list, per);
   const int plane = ny * hs;
+  int staged = -1;  // slot whose descriptor sdesc holds
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int k = udiv(item, g.fd_it_plane);
     const int local = item - k * per;
-    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc);
+    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc, staged);
     if (skip_item<TF, PRO>(S)) continue;
     const int x = udiv(local, g.fd_3);
     const int p = local - 3 * x;
@@ -933,7 +937,6 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     if constexpr (PRO_IS_KRYLOV(PRO)) {
       if (u.on) finish_pending_update(S, xx, local, per, red);
     }
-    __syncthreads();
   }
 }
 
@@ -955,11 +958,12 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
   const int per = items_plane(g);
   const int n_items = list_items(list, per);
   const int plane = ny * hs;
+  int staged = -1;  // slot whose descriptor sdesc holds
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int k = udiv(item, g.fd_it_plane);
     const int local = item - k * per;
-    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc);
-    if (EPI == EPI_MINRES && block_read_flag(&S.st->done)) continue;
+    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc, staged);
+    if (EPI == EPI_MINRES && slot_done(S.st)) continue;
     const int x = udiv(local, g.fd_3);
     const int p = local - 3 * x;
     const cplx<T> *spec = reinterpret_cast<const cplx<T> *>(S.spec);
@@ -988,7 +992,6 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
     plane_epilogue<T, TF, EPI>(S, io, V, (long long)x * ny * nz, ny * nz, p, fin, acc0, acc1, acc2);
     finish_inverse<TF, EPI>(S, acc0, acc1, acc2, local, per, red);
-    __syncthreads();
   }
 }
 
@@ -1051,10 +1054,11 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
   const int y0 = rank * R;
   const int cown = (rank * Lq) / hs, k0 = rank * Lq - cown * hs;  // owned columns
   const int ncl = gridDim.x / C;
+  int staged = -1;  // slot whose descriptor sdesc holds
   for (int item = blockIdx.x / C; item < n_items; item += ncl) {
     const int k = udiv(item, g.fd_it_plane);
     const int local = item - k * per;
-    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc);
+    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc, staged);
     const bool skip = skip_item<TF, PRO>(S);
     const int x = udiv(local, g.fd_3);
     const int p = local - 3 * x;
@@ -1099,7 +1103,6 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
         if (u.on) finish_pending_update(S, xx, local * C + rank, per * C, red);
       }
     }
-    __syncthreads();
   }
 }
 
@@ -1132,11 +1135,12 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
   const int lam0 = rank * Lq;
   const int cown = lam0 / hs, k0 = lam0 - cown * hs;
   const int ncl = gridDim.x / C;
+  int staged = -1;  // slot whose descriptor sdesc holds
   for (int item = blockIdx.x / C; item < n_items; item += ncl) {
     const int k = udiv(item, g.fd_it_plane);
     const int local = item - k * per;
-    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc);
-    const bool skip = (EPI == EPI_MINRES) && block_read_flag(&S.st->done);
+    const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc, staged);
+    const bool skip = (EPI == EPI_MINRES) && slot_done(S.st);
     const int x = udiv(local, g.fd_3);
     const int p = local - 3 * x;
     if (!skip) {
@@ -1183,6 +1187,5 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
                                  acc1, acc2);
       finish_inverse<TF, EPI>(S, acc0, acc1, acc2, local * C + rank, per * C, red);
     }
-    __syncthreads();
   }
 }

@@ -114,27 +114,22 @@ __device__ __forceinline__ bool last_item_arrives(unsigned int *ticket, unsigned
   return is_last;
 }
 
-// Block-uniform read of a slot flag (thread 0 reads, the block agrees).
-__device__ __forceinline__ int block_read_flag(const int *p) {
-  __shared__ int v;
-  __syncthreads();
-  if (threadIdx.x == 0) v = *(const volatile int *)p;
-  __syncthreads();
-  return v;
-}
-
 // Copy one slot's descriptor into shared memory (raw: sizeof(SlotDev<T>) bytes, 16-byte
-// aligned) and return it.  Pointers read from there occupy registers only where they are
-// used, not across a whole item; the block syncs before (the previous item is done with
-// the copy) and after.
+// aligned) unless it holds that slot already, and return it.  `staged` is the slot raw
+// holds (the same in every thread of the block; -1 at the start of a kernel); the
+// descriptors do not change during a launch.  Pointers read from there occupy registers
+// only where they are used, not across a whole item.  The block syncs around a copy.
 template <typename T>
 __device__ __forceinline__ const SlotDev<T> &stage_slot(const SlotDev<T> *tab, int slot,
-                                                        unsigned char *raw) {
-  __syncthreads();
-  const uint32_t *src = reinterpret_cast<const uint32_t *>(tab + slot);
-  uint32_t *dst = reinterpret_cast<uint32_t *>(raw);
-  for (int i = threadIdx.x; i < (int)(sizeof(SlotDev<T>) / 4); i += blockDim.x) dst[i] = src[i];
-  __syncthreads();
+                                                        unsigned char *raw, int &staged) {
+  if (slot != staged) {
+    __syncthreads();
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(tab + slot);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(raw);
+    for (int i = threadIdx.x; i < (int)(sizeof(SlotDev<T>) / 4); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    staged = slot;
+  }
   return *reinterpret_cast<const SlotDev<T> *>(raw);
 }
 
