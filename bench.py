@@ -581,6 +581,70 @@ def sweep_mode(args, w):
     print(json.dumps(out), flush=True)
 
 
+def classes_mode(args, w):
+    """Per class of the serving stream's first ``--count`` requests (default 64): the plain
+    single-request FP64 solve (one request at a time) against the served mixed solve of the
+    same requests (all submitted at once on a fresh server, the class alone on the GPU):
+    solves/s of each, their ratio, iteration totals and the stress error between them."""
+    from materialite_b200.serving import RVEServer, request_stream, run_stream, solve_plain
+    count = args.count or 64
+    reqs = request_stream(count, w["rate"], seed=w["seed"], workers=host_workers())
+    by = {}
+    for r in reqs:
+        by.setdefault(r.kind, []).append(r)
+    out = {"workload": f"first {count} requests of the serving stream, by class", "classes": {}}
+    for kind in sorted(by):
+        rs = by[kind]
+        secs, pouts = solve_plain(rs, precision="fp64", device=0, keep_stress=True)
+        ref = [r.stress.copy() for r in rs]
+        srv = RVEServer(device=0, max_slots=w["slots"], precision="mixed")
+        for r in rs:
+            r.keep_stress = True
+            r.arrival = 0.0
+        comps, span = run_stream(srv, rs, timeout=3600)
+        srv.close()
+        err = max(float(np.linalg.norm(r.stress - a) / np.linalg.norm(a)) for r, a in zip(rs, ref))
+        plain = len(rs) / float(sum(secs))
+        served = len(rs) / span
+        out["classes"][kind] = {
+            "count": len(rs), "plain_fp64_solves_per_s": plain, "served_solves_per_s": served,
+            "served_over_plain": served / plain,
+            "newton": int(sum(c.result.newton_iterations for c in comps)),
+            "krylov": int(sum(c.result.krylov_iterations for c in comps)),
+            "plain_newton": int(sum(o.newton_iterations for o in pouts)),
+            "plain_krylov": int(sum(o.krylov_iterations for o in pouts)),
+            "stress_rel_l2_max": err}
+        print(json.dumps({kind: out["classes"][kind]}), flush=True)
+    print(json.dumps(out), flush=True)
+
+
+def group_mode(args, w):
+    """The first ``--count`` requests of one class (``--kind``, e.g. evp64) of the serving
+    stream, all submitted at once to a fresh server: the class alone on the GPU, every
+    Krylov launch batching all of its slots (the case the batched kernels are profiled
+    on)."""
+    from materialite_b200.serving import RVEServer, request_kind, request_stream, run_stream
+    count = args.count or 16
+    tags, t = [], 0
+    while len(tags) < count and t < 100000:
+        if request_kind(t, seed=w["seed"])[0] == args.kind:
+            tags.append(t)
+        t += 1
+    reqs = request_stream(len(tags), w["rate"], seed=w["seed"], workers=host_workers(), tags=tags)
+    srv = RVEServer(device=0, max_slots=w["slots"], precision=args.precision)
+    for r in reqs:
+        r.arrival = 0.0
+    comps, span = run_stream(srv, reqs, timeout=3600)
+    launches = srv.kernel_launches()
+    srv.close()
+    print(json.dumps({"kind": args.kind, "count": len(reqs), "precision": args.precision,
+                      "solves_per_s": len(reqs) / span, "seconds": span,
+                      "newton": int(sum(c.result.newton_iterations for c in comps)),
+                      "krylov": int(sum(c.result.krylov_iterations for c in comps)),
+                      "kernel_launches": launches,
+                      "failed": sum(1 for c in comps if c.status != 0)}), flush=True)
+
+
 def request_mode(args, w):
     """One request of the serving stream (``--tag``), alone, in the chosen precision:
     the target of per-request kernel profiles."""
@@ -692,7 +756,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--mode", default="bench",
-                    choices=["bench", "kernels", "request", "accuracy", "sweep"],
+                    choices=["bench", "kernels", "request", "accuracy", "sweep", "classes",
+                             "group"],
                     help="kernels: one load increment, then the Krylov kernels timed in "
                          "isolation (the target of the ncu captures under profiles/); "
                          "request: one request of the serving stream alone; accuracy: one "
@@ -706,10 +771,17 @@ def main():
     ap.add_argument("--no-roofline", action="store_true")
     ap.add_argument("--tag", type=int, default=0, help="request mode: index in the stream")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--kind", default="evp64", help="group mode: request class (e.g. evp64)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.mode == "kernels":
         kernels_mode(args, w)
+        return
+    if args.mode == "classes":
+        classes_mode(args, WORKLOADS["serve"])
+        return
+    if args.mode == "group":
+        group_mode(args, WORKLOADS["serve"])
         return
     if args.mode == "accuracy":
         accuracy_mode(args, w)

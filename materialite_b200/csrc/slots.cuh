@@ -100,10 +100,12 @@ template <typename T> __device__ __forceinline__ KRoles<T> kroles(const SlotDev<
 
 // A slot's reduction: every item stores its partials, and the item that arrives last
 // (ticket == total - 1) sees all of them.  Returns true in every thread of that item's
-// block; the ticket is reset by the caller.
+// block; the ticket is reset by the caller.  Callers store their partials from the first
+// warp, which alone fences them before the ticket: a fence in every thread would wait for
+// all of the block's outstanding field stores.
 __device__ __forceinline__ bool last_item_arrives(unsigned int *ticket, unsigned int total) {
   __shared__ bool is_last;
-  __threadfence();
+  if (threadIdx.x < 32) __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned int t = atomicAdd(ticket, 1u);
