@@ -3,8 +3,11 @@
 // processors", SC 2008).  Every stage reads one buffer and writes the other, so a
 // transform of length N = r_1 r_2 ... r_m takes m stages and no bit reversal.
 //
-// Radices 2, 3, 4 and 8 have hand-written butterflies; any other factor (5, 7, ...,
-// up to SSFFT_MAX_GENERIC_RADIX) uses a direct DFT with the twiddle table.
+// Radices 2, 3, 4, 8, 12 and 16 have hand-written butterflies (12 and 16 composed in
+// registers from radix-3/4 butterflies and constant twiddles); any other factor (5, 7, ...,
+// up to SSFFT_MAX_GENERIC_RADIX) uses a direct DFT with the twiddle table.  A plan uses the
+// fewest stages its radices allow (every stage is a pass through shared memory), widest
+// radix first (the first stage needs no twiddles): 128 = 16 x 8, 96 = 12 x 8, 48 = 16 x 3.
 #pragma once
 
 #include "common.cuh"
@@ -42,28 +45,71 @@ struct AxisPlan {
   FastDiv nsdiv[SSFFT_MAX_STAGES];// divisor Ns = rad[0] * ... * rad[s-1]
 };
 
-// Factor n into stages: radix 8 first, then 4, 2, then odd factors (<= 32).
-static inline bool make_axis_plan(int n, AxisPlan &p) {
+// Factor n into stages with the fewest passes: radices up to `maxrad` among 16, 12, 8, 4,
+// 3, 2 (hand-written butterflies) and odd primes up to SSFFT_MAX_GENERIC_RADIX (direct
+// DFT).  Among plans of equal length: fewer generic stages, then the widest radix first.
+static inline void plan_search(int m, int maxrad, int *cur, int depth, int *best, int *best_len,
+                               int *best_gen) {
+  if (depth > SSFFT_MAX_STAGES) return;
+  if (m == 1) {
+    int gen = 0;  // stages without a hand-written butterfly
+    for (int i = 0; i < depth; ++i) {
+      const int r = cur[i];
+      gen += (r == 2 || r == 3 || r == 4 || r == 8 || r == 12 || r == 16) ? 0 : 1;
+    }
+    // sort descending (widest radix first)
+    int tmp[SSFFT_MAX_STAGES];
+    for (int i = 0; i < depth; ++i) tmp[i] = cur[i];
+    for (int i = 0; i < depth; ++i)
+      for (int j = i + 1; j < depth; ++j)
+        if (tmp[j] > tmp[i]) {
+          const int t = tmp[i];
+          tmp[i] = tmp[j];
+          tmp[j] = t;
+        }
+    bool better = *best_len < 0 || depth < *best_len || (depth == *best_len && gen < *best_gen);
+    if (!better && depth == *best_len && gen == *best_gen) {
+      for (int i = 0; i < depth; ++i) {
+        if (tmp[i] != best[i]) {
+          better = tmp[i] > best[i];
+          break;
+        }
+      }
+    }
+    if (better) {
+      for (int i = 0; i < depth; ++i) best[i] = tmp[i];
+      *best_len = depth;
+      *best_gen = gen;
+    }
+    return;
+  }
+  if (*best_len >= 0 && depth + 1 > *best_len) return;
+  static const int hand[6] = {16, 12, 8, 4, 3, 2};
+  for (int i = 0; i < 6; ++i) {
+    const int r = hand[i];
+    if (r > maxrad || m % r) continue;
+    cur[depth] = r;
+    plan_search(m / r, maxrad, cur, depth + 1, best, best_len, best_gen);
+  }
+  for (int f = 5; f <= SSFFT_MAX_GENERIC_RADIX; f += 2) {
+    bool prime = true;
+    for (int d = 3; d * d <= f; d += 2)
+      if (f % d == 0) prime = false;
+    if (!prime || m % f) continue;
+    cur[depth] = f;
+    plan_search(m / f, maxrad, cur, depth + 1, best, best_len, best_gen);
+  }
+}
+
+static inline bool make_axis_plan(int n, AxisPlan &p, int maxrad = 8) {
   p.n = n;
   p.nrad = 0;
-  int m = n;
-  auto push = [&](int r) {
-    if (p.nrad >= SSFFT_MAX_STAGES) return false;
-    p.rad[p.nrad++] = r;
-    m /= r;
-    return true;
-  };
-  while (m % 8 == 0)
-    if (!push(8)) return false;
-  while (m % 4 == 0)
-    if (!push(4)) return false;
-  while (m % 2 == 0)
-    if (!push(2)) return false;
-  for (int f = 3; m > 1; f += 2) {
-    while (m % f == 0) {
-      if (f > SSFFT_MAX_GENERIC_RADIX) return false;
-      if (!push(f)) return false;
-    }
+  int cur[SSFFT_MAX_STAGES + 1], best[SSFFT_MAX_STAGES + 1], best_len = -1, best_gen = 0;
+  if (n < 1) return false;
+  if (n > 1) {
+    plan_search(n, maxrad, cur, 0, best, &best_len, &best_gen);
+    if (best_len < 0) return false;
+    for (int i = 0; i < best_len; ++i) p.rad[p.nrad++] = best[i];
   }
   int ns = 1;
   for (int st = 0; st < p.nrad; ++st) {
@@ -157,6 +203,77 @@ __device__ __forceinline__ void bfly3(cplx<T> *v) {
   v[2] = csub<T>(m, r);
 }
 
+// Radix 16 as 4 x 4 in registers: DFT4 over n1 of x[4 n1 + n2] for each n2, twiddles
+// W16^(n2 k1), DFT4 over n2 for each k1 (output k1 + 4 k2).
+template <typename T, bool INV>
+__device__ __forceinline__ void bfly16(cplx<T> *v) {
+  const T c1 = (T)0.92387953251128675613;  // cos(pi/8)
+  const T s1 = (T)0.38268343236508977173;  // sin(pi/8)
+  const T h = (T)INV_SQRT2_D;
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) {
+    cplx<T> t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+    bfly4<T, INV>(t);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) v[4 * k1 + n2] = t[k1];  // A[n2][k1] at 4 k1 + n2
+  }
+  // W16^m = cos(pi m / 8) - i sin(pi m / 8) (conjugate for the inverse)
+  const T sg = INV ? (T)-1 : (T)1;
+  const cplx<T> w1 = mk<T>(c1, -sg * s1), w2 = mk<T>(h, -sg * h), w3 = mk<T>(s1, -sg * c1);
+  const cplx<T> w6 = mk<T>(-h, -sg * h), w9 = mk<T>(-c1, sg * s1);
+  v[4 * 1 + 1] = cmul<T>(v[4 * 1 + 1], w1);
+  v[4 * 2 + 1] = cmul<T>(v[4 * 2 + 1], w2);
+  v[4 * 3 + 1] = cmul<T>(v[4 * 3 + 1], w3);
+  v[4 * 1 + 2] = cmul<T>(v[4 * 1 + 2], w2);
+  v[4 * 2 + 2] = mul_mi<T, INV>(v[4 * 2 + 2]);  // W16^4 = -i
+  v[4 * 3 + 2] = cmul<T>(v[4 * 3 + 2], w6);
+  v[4 * 1 + 3] = cmul<T>(v[4 * 1 + 3], w3);
+  v[4 * 2 + 3] = cmul<T>(v[4 * 2 + 3], w6);
+  v[4 * 3 + 3] = cmul<T>(v[4 * 3 + 3], w9);
+  cplx<T> o[16];
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    cplx<T> t[4] = {v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]};
+    bfly4<T, INV>(t);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) o[k1 + 4 * k2] = t[k2];
+  }
+#pragma unroll
+  for (int q = 0; q < 16; ++q) v[q] = o[q];
+}
+
+// Radix 12 as 3 x 4 in registers: DFT3 over n1 of x[4 n1 + n2] for each n2, twiddles
+// W12^(n2 k1), DFT4 over n2 for each k1 (output k1 + 3 k2).
+template <typename T, bool INV>
+__device__ __forceinline__ void bfly12(cplx<T> *v) {
+  const T r3 = (T)0.86602540378443864676;  // sqrt(3)/2
+  cplx<T> a[12];
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) {
+    cplx<T> t[3] = {v[n2], v[4 + n2], v[8 + n2]};
+    bfly3<T, INV>(t);
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1) a[4 * k1 + n2] = t[k1];  // A[n2][k1] at 4 k1 + n2
+  }
+  // W12^m = cos(pi m / 6) - i sin(pi m / 6) (conjugate for the inverse)
+  const T sg = INV ? (T)-1 : (T)1;
+  const cplx<T> w1 = mk<T>(r3, -sg * (T)0.5), w2 = mk<T>((T)0.5, -sg * r3);
+  const cplx<T> w4 = mk<T>((T)-0.5, -sg * r3);
+  a[4 * 1 + 1] = cmul<T>(a[4 * 1 + 1], w1);
+  a[4 * 2 + 1] = cmul<T>(a[4 * 2 + 1], w2);
+  a[4 * 1 + 2] = cmul<T>(a[4 * 1 + 2], w2);
+  a[4 * 2 + 2] = cmul<T>(a[4 * 2 + 2], w4);
+  a[4 * 1 + 3] = mul_mi<T, INV>(a[4 * 1 + 3]);  // W12^3 = -i
+  a[4 * 2 + 3] = mk<T>(-a[4 * 2 + 3].x, -a[4 * 2 + 3].y);  // W12^6 = -1
+#pragma unroll
+  for (int k1 = 0; k1 < 3; ++k1) {
+    cplx<T> t[4] = {a[4 * k1], a[4 * k1 + 1], a[4 * k1 + 2], a[4 * k1 + 3]};
+    bfly4<T, INV>(t);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) v[k1 + 3 * k2] = t[k2];
+  }
+}
+
 // One Stockham stage of radix R (R = 0: generic radix r).  PAD: shared-memory indices go
 // through sidx<true>.
 template <typename T, bool INV, bool LINES_FAST, int R, bool PAD>
@@ -193,6 +310,8 @@ __device__ __forceinline__ void fft_stage(const cplx<T> *__restrict__ src,
       if (R == 3) bfly3<T, INV>(v);
       if (R == 4) bfly4<T, INV>(v);
       if (R == 8) bfly8<T, INV>(v);
+      if (R == 12) bfly12<T, INV>(v);
+      if (R == 16) bfly16<T, INV>(v);
 #pragma unroll
       for (int q = 0; q < R; ++q) dst[sidx<PAD>(base + (outj + q * Ns) * L.estride)] = v[q];
     } else {
@@ -227,6 +346,12 @@ __device__ cplx<T> *smem_fft(cplx<T> *a, cplx<T> *b, const LineLayout &L, const 
       case 3: fft_stage<T, INV, LINES_FAST, 3, PAD>(a, b, L, P.n, r, Ns, md, nd, tw); break;
       case 4: fft_stage<T, INV, LINES_FAST, 4, PAD>(a, b, L, P.n, r, Ns, md, nd, tw); break;
       case 8: fft_stage<T, INV, LINES_FAST, 8, PAD>(a, b, L, P.n, r, Ns, md, nd, tw); break;
+      case 12:  // float plans only: a double radix-12/16 butterfly does not fit 64 registers
+        if constexpr (sizeof(T) == 4) fft_stage<T, INV, LINES_FAST, 12, PAD>(a, b, L, P.n, r, Ns, md, nd, tw);
+        break;
+      case 16:
+        if constexpr (sizeof(T) == 4) fft_stage<T, INV, LINES_FAST, 16, PAD>(a, b, L, P.n, r, Ns, md, nd, tw);
+        break;
       default: fft_stage<T, INV, LINES_FAST, 0, PAD>(a, b, L, P.n, r, Ns, md, nd, tw); break;
     }
     __syncthreads();

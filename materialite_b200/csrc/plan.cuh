@@ -211,9 +211,12 @@ template <typename T> static void fill_grid(GridPlan &p) {
   g.hz = p.hz;
   g.V = p.V;
   g.S = p.S;
-  g.px = p.px;
-  g.py = p.py;
-  g.pz = p.pz;
+  // float transforms take radix 16 and 12 butterflies (two stages for every length up to
+  // 256 the solver uses); double ones stop at radix 8, whose registers fit 64 a thread
+  const int maxrad = sizeof(T) == 4 ? 16 : 8;
+  make_axis_plan(p.nx, g.px, maxrad);
+  make_axis_plan(p.ny, g.py, maxrad);
+  make_axis_plan(p.nz, g.pz, maxrad);
   const int k = sizeof(T) == 8 ? 1 : 0;
   g.twx = (const cplx<T> *)p.tw[k][0];
   g.twy = (const cplx<T> *)p.tw[k][1];

@@ -58,6 +58,7 @@ struct ssfft_handle {
   cudaGraphExec_t krylov_graph;  // one Krylov chunk, captured on first use
   cudaGraphExec_t krylov_loop;   // while node over the chunk: the whole solve on device
   bool use_graphs, use_device_loop;
+  bool debug_minres;             // SSFFT_DEBUG_MINRES=1: each solve's stop reason to stderr
   int chunk_kernels;             // kernels launched by one chunk
   bool committed_view;           // last call was a commit: outputs read committed buffers
   double *h_results;             // pinned mirrors
@@ -216,6 +217,14 @@ template <typename T> static int run_minres(ssfft_handle *h, long long *iters) {
   }
   if (h->h_st->istop == 9) return fail(SSFFT_E_NAN, "non-finite value in the Krylov solve");
   *iters = h->h_st->itn;
+  if (h->debug_minres) {
+    const MinresState &s = *h->h_st;
+    fprintf(stderr,
+            "ssfft minres: itn %lld istop %d test1 %.3e test2 %.3e rnorm %.3e anorm %.3e "
+            "ynorm %.3e beta1 %.3e acond %.3e\n",
+            s.itn, s.istop, s.test1, s.test2, s.rnorm, s.anorm, s.ynorm, s.beta1,
+            s.gmin > 0 ? s.gmax / s.gmin : 0.0);
+  }
   return 0;
 }
 
@@ -442,6 +451,8 @@ extern "C" int ssfft_create(const ssfft_config *cfg, ssfft_handle **out) {
     h->use_graphs = !(ng && ng[0] == '1');
     const char *nl = getenv("SSFFT_NO_DEVICE_LOOP");
     h->use_device_loop = h->use_graphs && !(nl && nl[0] == '1');
+    const char *dm = getenv("SSFFT_DEBUG_MINRES");
+    h->debug_minres = dm && dm[0] == '1';
   }
   auto body = [&]() -> int {
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
