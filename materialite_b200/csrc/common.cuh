@@ -42,6 +42,20 @@ template <typename T, bool INV> __device__ __forceinline__ cplx<T> mul_mi(cplx<T
   return INV ? mk<T>(-a.y, a.x) : mk<T>(a.y, -a.x);
 }
 
+// ---- asynchronous global-to-shared copies -------------------------------------------
+// cp.async moves an element from global to shared memory without a register round trip, so
+// a thread can have all of a tile's loads in flight at once (a load-then-store loop waits a
+// full memory latency per element).  The caller waits with cp_async_wait_all() and then
+// syncs the block.
+template <typename T> __device__ __forceinline__ void cp_async_elem(cplx<T> *dst, const cplx<T> *src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(cplx<T>) == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // ---- block reductions (double) ------------------------------------------------------
 
 __device__ __forceinline__ double warp_sum(double v) {

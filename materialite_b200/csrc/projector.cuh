@@ -564,8 +564,9 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     __syncthreads();
     for (int e = threadIdx.x; e < ny * nk; e += blockDim.x) {
       const int y = udiv(e, g.fd_ky[ti]), kk = e - y * nk;
-      bufA[y * nk + kk] = base[(long long)y * hs + kk];
+      cp_async_elem<T>(&bufA[y * nk + kk], &base[(long long)y * hs + kk]);
     }
+    cp_async_wait_all();
     __syncthreads();
     const LineLayout L(nk, nk, 0, 1, nk, g.fd_ky[ti], g.fd_ky[ti]);
     cplx<T> *res = smem_fft<T, INV, true>(bufA, bufB, L, g.py, tw);
@@ -651,8 +652,9 @@ __global__ void __launch_bounds__(XPASS_THREADS)
     for (int e = threadIdx.x; e < 6 * slab; e += blockDim.x) {
       const int c = udiv(e, g.fd_xslab[ti]), rem = e - c * slab;
       const int x = udiv(rem, g.fd_kx[ti]), kk = rem - x * nk;
-      bufA[c * sst + x * nk + kk] = spec[c * g.S + ((long long)x * ny + y) * hs + k0 + kk];
+      cp_async_elem<T>(&bufA[c * sst + x * nk + kk], &spec[c * g.S + ((long long)x * ny + y) * hs + k0 + kk]);
     }
+    cp_async_wait_all();
     __syncthreads();
     const LineLayout L(6 * nk, nk, sst, 1, nk, g.fd_x6k[ti], g.fd_kx[ti]);
     cplx<T> *res = smem_fft<T, false, true>(bufA, bufB, L, g.px, tw);
@@ -731,7 +733,19 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
       }
     }
     const cplx<T> *spec = reinterpret_cast<const cplx<T> *>(S.spec);
+    const int hs = g.hs, nlhs = nl * hs;
     __syncthreads();
+    // the tile's stored halves, [c][l][ks] in bufB, all in flight at once (the tile's lines
+    // are consecutive rows of the spectrum)
+    const bool staged_half = 6 * nlhs <= zbuf_elems(g.lz, nz);
+    if (staged_half) {
+      for (int e = threadIdx.x; e < 6 * nlhs; e += blockDim.x) {
+        const int c = udiv(e, g.fd_znh[ti]), rem = e - c * nlhs;
+        cp_async_elem<T>(&bufB[e], &spec[c * g.S + line0 * hs + rem]);
+      }
+      cp_async_wait_all();
+      __syncthreads();
+    }
     // rebuild the full z spectrum of Z = A + iB from the stored half (Hermitian in z)
     for (int e = threadIdx.x; e < 3 * nel; e += blockDim.x) {
       const int p = udiv(e, g.fd_znz[ti]);
@@ -739,10 +753,18 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
       const int l = udiv(rem, g.fd_nz), kk = rem - l * nz;
       const bool low = (kk < hz);
       const int ks = low ? kk : nz - kk;
-      const long long off = (line0 + l) * g.hs + ks;
       const bool nyq = 2 * ks == nz;  // the unstored Nyquist column is zero
-      const cplx<T> A = nyq ? mk<T>((T)0, (T)0) : spec[(2 * p) * g.S + off];
-      const cplx<T> B = nyq ? mk<T>((T)0, (T)0) : spec[(2 * p + 1) * g.S + off];
+      cplx<T> A = mk<T>((T)0, (T)0), B = A;
+      if (!nyq) {
+        if (staged_half) {
+          A = bufB[(2 * p) * nlhs + l * hs + ks];
+          B = bufB[(2 * p + 1) * nlhs + l * hs + ks];
+        } else {
+          const long long off = (line0 + l) * hs + ks;
+          A = spec[(2 * p) * g.S + off];
+          B = spec[(2 * p + 1) * g.S + off];
+        }
+      }
       bufA[sidx<true>((p * nl + l) * nz + kk)] =
           low ? mk<T>(A.x - B.y, A.y + B.x) : mk<T>(A.x + B.y, B.x - A.y);
     }
@@ -970,8 +992,9 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     __syncthreads();
     for (int e = threadIdx.x; e < 2 * plane; e += blockDim.x) {
       const int c = udiv(e, g.fd_plane), rem = e - c * plane;
-      bufA[e] = spec[(2 * p + c) * g.S + (long long)x * plane + rem];
+      cp_async_elem<T>(&bufA[e], &spec[(2 * p + c) * g.S + (long long)x * plane + rem]);
     }
+    cp_async_wait_all();
     __syncthreads();
     const LineLayout Ly(2 * hs, hs, plane, 1, hs, g.fd_2hs, g.fd_hs);
     cplx<T> *res = smem_fft<T, true, true>(bufA, bufB, Ly, g.py, twy);
@@ -1149,8 +1172,9 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
       __syncthreads();
       for (int e = threadIdx.x; e < ny * Lq; e += blockDim.x) {
         const int y = udiv(e, cq.fd_Lq), kl = e - y * Lq;
-        bufA[e] = spec[(long long)y * hs + kl];
+        cp_async_elem<T>(&bufA[e], &spec[(long long)y * hs + kl]);
       }
+      cp_async_wait_all();
       __syncthreads();
       const LineLayout Ly(Lq, Lq, 0, 1, Lq, cq.fd_Lq, cq.fd_Lq);
       smem_fft<T, true, true>(bufA, bufB, Ly, g.py, twy);
