@@ -84,21 +84,22 @@ def plane_path(n):
 
 # Algorithmic HBM bytes per voxel of each Krylov-iteration kernel with float fields:
 # planar vectors are 24 B/voxel (6 x 4 B); the stored half spectrum is 6 x hs/n x 8 B with
-# hs = n/2 columns on even grids (the zeroed Nyquist column is not stored), (n+1)/2 on odd.  The
-# forward z pass also applies the previous iteration's vector update (reads y', u, w1,
-# w2, x; writes u', w, x).  With the plane-fused passes the y transforms happen in shared
-# memory inside the z kernels and move no bytes of their own.
+# hs = n/2 columns on even grids (the zeroed Nyquist column is not stored), (n+1)/2 on odd.
+# The update kernel applies the previous iteration's vector update (reads y', u, w1, w2, x;
+# writes u', w, x) and writes tau = K v over y'; the forward z pass reads tau and writes the
+# spectrum.  With the plane-fused passes the y transforms happen in shared memory inside
+# the z kernels and move no bytes of their own.
 def kernel_bytes_per_voxel(n, table_mode=True):
     spec = 6 * (n // 2 if n % 2 == 0 else n // 2 + 1) / n * 8.0
     kin = 4.0 if table_mode else 84.0
     ypass = 0.0 if plane_path(n) else 2 * spec
     return {
-        "zfwd": 8 * 24.0 + kin + spec,      # update vectors, tangent; write spectrum
+        "zfwd": 24.0 + spec,                # read tau; write spectrum
         "yfwd": ypass,
         "xpass": 2 * spec,                  # read + write spectrum
         "yinv": ypass,
         "zinv": spec + 3 * 24.0,            # read spectrum, u_{j-1}, u_j; write y'
-        "update": 0.0,                      # fused into the forward z pass
+        "update": 8 * 24.0 + kin + 24.0,    # update vectors, tangent; write tau
     }
 
 

@@ -4,21 +4,21 @@
 //
 // All scalars live in a MinresState in device memory (one per slot) and are advanced by
 // the last item of each reduction, so an iteration needs no host round trip.  With u_j
-// the Lanczos vector of iteration j (v_j = u_j / beta_j), one iteration is three
-// (plane-fused) or five kernels:
+// the Lanczos vector of iteration j (v_j = u_j / beta_j), one iteration is four
+// (plane-fused) or six kernels:
 //
-//   forward z(y)  pending update of iteration j-1: u_j = y' - (alfa/beta) u_{j-1},
+//   update        pending update of iteration j-1: u_j = y' - (alfa/beta) u_{j-1},
 //                 w = (v_{j-1} - oldeps w1 - delta w2) / gamma, x += phi w;
 //                 last item: |x| and the stopping tests          (minres_after_update)
-//                 then tau = K (u_j / beta_j) and its forward transform
+//                 then tau = K (u_j / beta_j) into y''s buffer
+//   forward z(y)  forward transform of tau
 //   ... y/x passes ...
 //   inverse z     y' = P tau - (beta_j / beta_{j-1}) u_{j-1}; u_j.y', y'.y', u_j.u_j;
 //                 last item: alfa, beta_{j+1}, plane rotation    (minres_after_matvec)
 //
 // The update needs alfa, a global dot product of the matvec, so it cannot join the
-// inverse pass; it rides on the next forward pass, which reads the same vectors anyway.
-// The last iteration's update is applied by one more forward pass, which then finds the
-// solve done.  Vectors are component-planar in the solve precision T, handled as one
+// inverse pass; it opens the next iteration.  The last iteration's update is applied by
+// one more update pass, which then finds the solve done.  Vectors are component-planar in the solve precision T, handled as one
 // contiguous run of 6V values; every dot product and norm accumulates in double, in a
 // fixed order (item partials summed by the slot's last item), so results depend neither on
 // scheduling nor on the other slots of a launch.  Buffer roles follow the slot's own
@@ -104,6 +104,41 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
       }
     }
     __syncthreads();
+  }
+}
+
+// The forward half of a Krylov matvec, elementwise: for every listed slot whose solve is
+// not done, the pending update of the previous iteration (u_j = y' - coef u_{j-1}, w, x,
+// |x|^2 and, in the slot's last item, the stopping tests) and tau = K (s u_j), which
+// replaces y' in its buffer point by point (y' is consumed here; the inverse pass of this
+// iteration writes the next y' there).  The forward transform then copies tau from there
+// (PRO_TAU).  A plain streaming kernel: each point's loads go out together and no register
+// cap is imposed, so the loads of a block keep HBM busy.
+template <typename T, int PRO>
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    krylov_update_kernel(const SlotDev<T> *__restrict__ tab, SlotList list, long long V) {
+  __shared__ double red[32];
+  __shared__ __align__(16) unsigned char sdesc[sizeof(SlotDev<T>)];
+  const int per = vec_items(V);
+  const int n_items = list_items(list, per);
+  int staged = -1;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int k = item / per;
+    const int local = item - k * per;
+    const SlotDev<T> &S = stage_slot<T>(tab, list.ids[k], sdesc, staged);
+    if (slot_done(S.st)) continue;
+    const KrylovIn<T, T> u = krylov_in<T, T>(S);
+    const long long v0 = (long long)local * VEC_CHUNK;
+    const long long v1 = min(V, v0 + VEC_CHUNK);
+    T *tau_out = u.r.Y;
+    double xx = 0.0;
+    for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
+      T tau[6];
+      tangent_prologue<T, T, PRO, true>(S, V, v, u, 0, tau, xx);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) tau_out[c * V + v] = tau[c];
+    }
+    if (u.on) finish_pending_update(S, xx, local, per, red);
   }
 }
 

@@ -417,8 +417,7 @@ template <typename T, typename TF, int PT> static int plane_attrs(int m) {
   CKR(smem_attr(yzinv_kernel<T, TF, EPI_RESIDUAL, PT>, m));
   CKR(smem_attr(yzinv_kernel<T, TF, EPI_REPROJECT, PT>, m));
   if (sizeof(T) == sizeof(TF)) {
-    CKR(smem_attr(zyfwd_kernel<T, T, PRO_TANGENT_TABLE, PT>, m));
-    CKR(smem_attr(zyfwd_kernel<T, T, PRO_TANGENT_VOXEL, PT>, m));
+    CKR(smem_attr(zyfwd_kernel<T, T, PRO_TAU, PT>, m));
     CKR(smem_attr(yzinv_kernel<T, T, EPI_MINRES, PT>, m));
   }
   return 0;
@@ -432,8 +431,7 @@ template <typename T, typename TF, int PT> static int cluster_attrs(int m) {
   CKR(smem_attr(yzinv_cl_kernel<T, TF, EPI_RESIDUAL, PT>, m));
   CKR(smem_attr(yzinv_cl_kernel<T, TF, EPI_REPROJECT, PT>, m));
   if (sizeof(T) == sizeof(TF)) {
-    CKR(smem_attr(zyfwd_cl_kernel<T, T, PRO_TANGENT_TABLE, PT>, m));
-    CKR(smem_attr(zyfwd_cl_kernel<T, T, PRO_TANGENT_VOXEL, PT>, m));
+    CKR(smem_attr(zyfwd_cl_kernel<T, T, PRO_TAU, PT>, m));
     CKR(smem_attr(yzinv_cl_kernel<T, T, EPI_MINRES, PT>, m));
   }
   return 0;
@@ -460,8 +458,7 @@ template <typename T, typename TF> static int set_kernel_attrs(size_t smax) {
   CKR((cluster_attrs<T, TF, 1024>(m)));
   if (sizeof(T) == sizeof(TF)) {
     CKR(smem_attr(constitutive_kernel<T>, (int)constitutive_smem_bytes()));
-    CKR(smem_attr(zfwd_kernel<T, T, PRO_TANGENT_TABLE>, m));
-    CKR(smem_attr(zfwd_kernel<T, T, PRO_TANGENT_VOXEL>, m));
+    CKR(smem_attr(zfwd_kernel<T, T, PRO_TAU>, m));
     CKR(smem_attr(zinv_kernel<T, T, EPI_MINRES>, m));
   }
   return 0;
@@ -922,11 +919,22 @@ static int launch_projector(const LaunchCtx &c, const SlotDev<TF> *tab, ExtIO<TF
 // One MINRES iteration on every listed slot whose solve is not done: the projector passes
 // with the pending vector update in the forward prologue and the scalar recurrence in the
 // inverse epilogue.
+// ev (optional, 8 events): ev[7] before the update kernel, ev[0..5] by the projector.
 template <typename T>
 static int launch_krylov_iteration(const LaunchCtx &c, const SlotDev<T> *tab, bool voxel,
                                    cudaEvent_t *ev = nullptr) {
-  if (voxel) return launch_projector<T, T, PRO_TANGENT_VOXEL, EPI_MINRES>(c, tab, {}, ev);
-  return launch_projector<T, T, PRO_TANGENT_TABLE, EPI_MINRES>(c, tab, {}, ev);
+  if (ev) cudaEventRecord(ev[7], c.stream);
+  const long long it = (long long)c.cap * vec_items(c.p->V);
+  if (voxel) {
+    auto k = krylov_update_kernel<T, PRO_TANGENT_VOXEL>;
+    k<<<persistent_grid(k, SSFFT_THREADS, 0, it, c.p->dev), SSFFT_THREADS, 0, c.stream>>>(tab, c.list, c.p->V);
+  } else {
+    auto k = krylov_update_kernel<T, PRO_TANGENT_TABLE>;
+    k<<<persistent_grid(k, SSFFT_THREADS, 0, it, c.p->dev), SSFFT_THREADS, 0, c.stream>>>(tab, c.list, c.p->V);
+  }
+  if (c.launches) *c.launches += 1;
+  CK(cudaGetLastError());
+  return launch_projector<T, T, PRO_TAU, EPI_MINRES>(c, tab, {}, ev);
 }
 
 // b = P(Sbar - sigma) into each slot's b, max|b| into results[40].  The transform always

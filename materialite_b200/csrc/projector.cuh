@@ -145,10 +145,13 @@ template <typename TF> struct ExtIO {
 // ---- prologue modes of the forward passes ---------------------------------------------
 //   PRO_INPUT          tau = caller's planes
 //   PRO_RESIDUAL       tau = Sbar - sigma                    (small_strain_fft.py:140,168)
-//   PRO_TANGENT_*      tau = K v of the Krylov iteration     (:370-374), table or voxel K
+//   PRO_TANGENT_*      tau = K v of the Krylov iteration     (:370-374), table or voxel K;
+//                      formed by the update kernel (krylov.cuh), not by a transform pass
 //   PRO_REPROJECT      tau = x (the Newton correction)
+//   PRO_TAU            tau = K v as the update kernel left it in the slot's y' buffer (the
+//                      forward transform of a Krylov iteration; skips finished solves)
 enum { PRO_INPUT = 0, PRO_RESIDUAL = 1, PRO_TANGENT_TABLE = 2, PRO_TANGENT_VOXEL = 3,
-       PRO_REPROJECT = 4 };
+       PRO_REPROJECT = 4, PRO_TAU = 5 };
 #define PRO_IS_KRYLOV(P) ((P) == PRO_TANGENT_TABLE || (P) == PRO_TANGENT_VOXEL)
 
 // ---- epilogue modes of the inverse passes -----------------------------------------------
@@ -390,7 +393,7 @@ __device__ __forceinline__ void load_table(cplx<T> *dst, const cplx<T> *src, int
 
 // Block-uniform "skip this item": a Krylov item of a slot whose solve is done.
 template <typename TF, int PRO> __device__ __forceinline__ bool skip_item(const SlotDev<TF> &S) {
-  if constexpr (PRO_IS_KRYLOV(PRO)) return slot_done(S.st);
+  if constexpr (PRO == PRO_TAU) return slot_done(S.st);
   return false;
 }
 
@@ -495,21 +498,32 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
     const long long line0 = (long long)local * g.lz;
     const int nl = (int)min((long long)g.lz, nlines_all - line0);
     const int ti = (nl == g.lz) ? 0 : 1;
-    KrylovIn<T, TF> u{};
-    if constexpr (PRO_IS_KRYLOV(PRO)) u = krylov_in<T, TF>(S);
-    double xx = 0.0;
     __syncthreads();  // table loaded; previous item done with the buffers
-    for (int e = threadIdx.x; e < nl * nz; e += blockDim.x) {
-      const int l = udiv(e, g.fd_nz), z = e - l * nz;
-      const long long v = (line0 + l) * nz + z;
-      T tau[6];
-      if constexpr (PRO_IS_KRYLOV(PRO))
-        tangent_prologue<T, TF, PRO, true>(S, V, v, u, 0, tau, xx);
-      else
+    if constexpr (PRO == PRO_TAU) {
+      // the six tau planes of the tile's lines straight into the paired lines, in flight
+      // together
+      const T *src = reinterpret_cast<const T *>(kroles<TF>(S, S.st->itn).Y);
+      for (int e = threadIdx.x; e < nl * nz; e += blockDim.x) {
+        const int l = udiv(e, g.fd_nz), z = e - l * nz;
+        const long long v = (line0 + l) * nz + z;
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          cplx<T> *d = &bufA[sidx<true>((p * nl + l) * nz + z)];
+          cp_async_scalar<T>(&d->x, src + (2 * p) * V + v);
+          cp_async_scalar<T>(&d->y, src + (2 * p + 1) * V + v);
+        }
+      }
+      cp_async_wait_all();
+    } else {
+      for (int e = threadIdx.x; e < nl * nz; e += blockDim.x) {
+        const int l = udiv(e, g.fd_nz), z = e - l * nz;
+        const long long v = (line0 + l) * nz + z;
+        T tau[6];
         prologue<T, TF, PRO>(S, io.in, V, v, tau);
 #pragma unroll
-      for (int p = 0; p < 3; ++p)
-        bufA[sidx<true>((p * nl + l) * nz + z)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
+        for (int p = 0; p < 3; ++p)
+          bufA[sidx<true>((p * nl + l) * nz + z)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
+      }
     }
     __syncthreads();
     const LineLayout L(3 * nl, 3 * nl, 0, nz, 1, g.fd_z3[ti], g.fd_z3[ti]);
@@ -528,9 +542,6 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
       const long long off = (line0 + l) * hs + kk;
       spec[(2 * p) * g.S + off] = A;
       spec[(2 * p + 1) * g.S + off] = B;
-    }
-    if constexpr (PRO_IS_KRYLOV(PRO)) {
-      if (u.on) finish_pending_update(S, xx, local, per, red);
     }
   }
 }
@@ -827,17 +838,23 @@ template <typename T> inline size_t smem_plane_bytes(int ny, int nz) {
 
 // Prologue of a plane item over the points vbase .. vbase + nel - 1 (whole z lines): tau
 // of the component pair p as one complex value per point, into padded z lines in buf.
+// PRO_TAU copies the pair's two planes with cp.async (all in flight at once).
 template <typename T, typename TF, int PRO>
 __device__ __forceinline__ void plane_prologue(const SlotDev<TF> &S, const ExtIO<TF> &io,
                                                long long V, long long vbase, int nel, int p,
-                                               const KrylovIn<T, TF> &u, cplx<T> *buf,
-                                               double &xx) {
-  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-    T tau[6];
-    if constexpr (PRO_IS_KRYLOV(PRO)) {
-      tangent_prologue<T, TF, PRO, false>(S, V, vbase + e, u, p, tau, xx);
-      buf[sidx<true>(e)] = mk<T>(tau[0], tau[1]);
-    } else {
+                                               cplx<T> *buf) {
+  if constexpr (PRO == PRO_TAU) {
+    const T *src = reinterpret_cast<const T *>(kroles<TF>(S, S.st->itn).Y);
+    const T *s0 = src + (2 * p) * V + vbase, *s1 = src + (2 * p + 1) * V + vbase;
+    for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+      cplx<T> *d = &buf[sidx<true>(e)];
+      cp_async_scalar<T>(&d->x, s0 + e);
+      cp_async_scalar<T>(&d->y, s1 + e);
+    }
+    cp_async_wait_all();
+  } else {
+    for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+      T tau[6];
       prologue<T, TF, PRO>(S, io.in, V, vbase + e, tau);
       buf[sidx<true>(e)] = mk<T>(tau[2 * p], tau[2 * p + 1]);
     }
@@ -929,12 +946,9 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     if (skip_item<TF, PRO>(S)) continue;
     const int x = udiv(local, g.fd_3);
     const int p = local - 3 * x;
-    KrylovIn<T, TF> u{};
-    if constexpr (PRO_IS_KRYLOV(PRO)) u = krylov_in<T, TF>(S);
-    double xx = 0.0;
     const long long vbase = (long long)x * ny * nz;
     __syncthreads();
-    plane_prologue<T, TF, PRO>(S, io, V, vbase, ny * nz, p, u, bufA, xx);
+    plane_prologue<T, TF, PRO>(S, io, V, vbase, ny * nz, p, bufA);
     __syncthreads();
     const LineLayout Lz(ny, ny, 0, nz, 1, g.fd_ny, g.fd_ny);
     cplx<T> *res = smem_fft<T, false, false, true>(bufA, bufB, Lz, g.pz, twz);
@@ -955,9 +969,6 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     for (int e = threadIdx.x; e < 2 * plane; e += blockDim.x) {
       const int c = udiv(e, g.fd_plane), rem = e - c * plane;
       spec[(2 * p + c) * g.S + (long long)x * plane + rem] = out[e];
-    }
-    if constexpr (PRO_IS_KRYLOV(PRO)) {
-      if (u.on) finish_pending_update(S, xx, local, per, red);
     }
   }
 }
@@ -1085,12 +1096,9 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     const bool skip = skip_item<TF, PRO>(S);
     const int x = udiv(local, g.fd_3);
     const int p = local - 3 * x;
-    KrylovIn<T, TF> u{};
-    if constexpr (PRO_IS_KRYLOV(PRO)) u = krylov_in<T, TF>(S);
-    double xx = 0.0;
     if (!skip) {
       __syncthreads();
-      plane_prologue<T, TF, PRO>(S, io, V, ((long long)x * ny + y0) * nz, R * nz, p, u, bufA, xx);
+      plane_prologue<T, TF, PRO>(S, io, V, ((long long)x * ny + y0) * nz, R * nz, p, bufA);
       __syncthreads();
       const LineLayout Lz(R, R, 0, nz, 1, cq.fd_R, cq.fd_R);
       smem_fft<T, false, false, true>(bufA, bufB, Lz, g.pz, twz);
@@ -1121,9 +1129,6 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
       for (int e = threadIdx.x; e < ny * Lq; e += blockDim.x) {
         const int y = udiv(e, cq.fd_Lq), kl = e - y * Lq;
         spec[(long long)y * hs + kl] = out[e];
-      }
-      if constexpr (PRO_IS_KRYLOV(PRO)) {
-        if (u.on) finish_pending_update(S, xx, local * C + rank, per * C, red);
       }
     }
   }

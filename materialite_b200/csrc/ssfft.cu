@@ -925,13 +925,16 @@ template <typename T> static int profile_impl(ssfft_handle *h, int reps, double 
     CK(cudaEventRecord(h->pev[6], h->stream));
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(h->pev[6]));
-    for (int i = 0; i < 6; ++i) {
+    // pev[7]: before the update kernel; pev[0..5]: the projector's pass slots
+    for (int i = 0; i < 5; ++i) {
       float ms = 0.f;
       CK(cudaEventElapsedTime(&ms, h->pev[i], h->pev[i + 1]));
       acc[i] += ms * 1e-3;
     }
     float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, h->pev[0], h->pev[6]));
+    CK(cudaEventElapsedTime(&ms, h->pev[7], h->pev[0]));
+    acc[5] += ms * 1e-3;
+    CK(cudaEventElapsedTime(&ms, h->pev[7], h->pev[6]));
     acc[7] += ms * 1e-3;
   }
   for (int i = 0; i < 8; ++i) sec[i] = acc[i] / reps;
