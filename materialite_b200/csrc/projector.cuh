@@ -478,7 +478,6 @@ template <typename T, typename TF, int PRO>
 __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
     zfwd_kernel(Grid<T> g, const SlotDev<TF> *__restrict__ tab, SlotList list, ExtIO<TF> io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double red[32];
   __shared__ __align__(16) unsigned char sdesc[sizeof(SlotDev<TF>)];
   const int nz = g.nz, hs = g.hs;
   const long long V = g.V;
@@ -924,7 +923,6 @@ template <typename T, typename TF, int PRO, int PT>
 __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     zyfwd_kernel(Grid<T> g, const SlotDev<TF> *__restrict__ tab, SlotList list, ExtIO<TF> io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double red[32];
   __shared__ __align__(16) unsigned char sdesc[sizeof(SlotDev<TF>)];
   const int ny = g.ny, nz = g.nz, hs = g.hs;
   const long long V = g.V;
@@ -1066,7 +1064,6 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
                     SlotList list, ExtIO<TF> io) {
   namespace cg = cooperative_groups;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double red[32];
   __shared__ __align__(16) unsigned char sdesc[sizeof(SlotDev<TF>)];
   cg::cluster_group cl = cg::this_cluster();
   const int C = cq.C, R = cq.R, Lq = cq.Lq;
