@@ -87,8 +87,9 @@ def plane_path(n):
 # hs = n/2 columns on even grids (the zeroed Nyquist column is not stored), (n+1)/2 on odd.
 # The update kernel applies the previous iteration's vector update (reads y', u, w1, w2, x;
 # writes u', w, x) and writes tau = K v over y'; the forward z pass reads tau and writes the
-# spectrum.  With the plane-fused passes the y transforms happen in shared memory inside
-# the z kernels and move no bytes of their own.
+# spectrum; the inverse z pass writes P tau over y', which the epilogue kernel turns into
+# y' (with the MINRES dot products).  With the plane-fused passes the y transforms happen in
+# shared memory inside the z kernels and move no bytes of their own.
 def kernel_bytes_per_voxel(n, table_mode=True):
     spec = 6 * (n // 2 if n % 2 == 0 else n // 2 + 1) / n * 8.0
     kin = 4.0 if table_mode else 84.0
@@ -98,12 +99,13 @@ def kernel_bytes_per_voxel(n, table_mode=True):
         "yfwd": ypass,
         "xpass": 2 * spec,                  # read + write spectrum
         "yinv": ypass,
-        "zinv": spec + 3 * 24.0,            # read spectrum, u_{j-1}, u_j; write y'
+        "zinv": spec + 24.0,                # read spectrum; write P tau
         "update": 8 * 24.0 + kin + 24.0,    # update vectors, tangent; write tau
+        "epilogue": 4 * 24.0,               # read P tau, u_{j-1}, u_j; write y'
     }
 
 
-KERNEL_NAMES = ["zfwd", "yfwd", "xpass", "yinv", "zinv", "update"]
+KERNEL_NAMES = ["zfwd", "yfwd", "xpass", "yinv", "zinv", "update", "epilogue"]
 
 
 def cubic_mandel(C11, C12, C44):

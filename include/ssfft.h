@@ -319,10 +319,11 @@ int ssfft_timer(ssfft_handle *h, int start, double *seconds);
 /* Kernel timing for roofline reports: runs `reps` Krylov iterations' kernels in
  * isolation on the handle's current tangent (the MINRES buffers are overwritten) and
  * returns the mean seconds per launch of each kernel, measured with CUDA events:
- * seconds[0..4] = zfwd (forward transform of tau), yfwd, xpass, yinv, zinv (MINRES
- * epilogue); the y slots are ~0 when the plane-fused passes run the y transforms inside
- * the z kernels; [5] = the update kernel (the previous iteration's vector update and
- * tau = K v); [6] = 0 (unused); [7] = one whole Krylov iteration timed back to back.
+ * seconds[0..4] = zfwd (forward transform of tau), yfwd, xpass, yinv, zinv (inverse
+ * transform, P tau stored); the y slots are ~0 when the plane-fused passes run the y
+ * transforms inside the z kernels; [5] = the update kernel (the previous iteration's vector
+ * update and tau = K v); [6] = the epilogue kernel (y' and the MINRES dot products);
+ * [7] = one whole Krylov iteration timed back to back.
  * The microstructure must be set and a solve must have run (non-uniform stress). */
 int ssfft_profile_krylov(ssfft_handle *h, int reps, double seconds[8]);
 

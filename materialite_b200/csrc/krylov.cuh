@@ -4,8 +4,8 @@
 //
 // All scalars live in a MinresState in device memory (one per slot) and are advanced by
 // the last item of each reduction, so an iteration needs no host round trip.  With u_j
-// the Lanczos vector of iteration j (v_j = u_j / beta_j), one iteration is four
-// (plane-fused) or six kernels:
+// the Lanczos vector of iteration j (v_j = u_j / beta_j), one iteration is five
+// (plane-fused) or seven kernels:
 //
 //   update        pending update of iteration j-1: u_j = y' - (alfa/beta) u_{j-1},
 //                 w = (v_{j-1} - oldeps w1 - delta w2) / gamma, x += phi w;
@@ -13,7 +13,8 @@
 //                 then tau = K (u_j / beta_j) into y''s buffer
 //   forward z(y)  forward transform of tau
 //   ... y/x passes ...
-//   inverse z     y' = P tau - (beta_j / beta_{j-1}) u_{j-1}; u_j.y', y'.y', u_j.u_j;
+//   inverse z     inverse transform: P tau into y''s buffer
+//   epilogue      y' = P tau - (beta_j / beta_{j-1}) u_{j-1}; u_j.y', y'.y', u_j.u_j;
 //                 last item: alfa, beta_{j+1}, plane rotation    (minres_after_matvec)
 //
 // The update needs alfa, a global dot product of the matvec, so it cannot join the
@@ -139,6 +140,49 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
       for (int c = 0; c < 6; ++c) tau_out[c * V + v] = tau[c];
     }
     if (u.on) finish_pending_update(S, xx, local, per, red);
+  }
+}
+
+// The MINRES half of the matvec epilogue, elementwise: over the P tau that the inverse
+// transform left in y''s buffer (EPI_PTAU), y' = P tau - (beta_j / beta_{j-1}) u_{j-1} in
+// place, and the dot products u_j.y', y'.y', u_j.u_j; the slot's last item advances the
+// recurrence (minres_after_matvec).
+template <typename T>
+__global__ void __launch_bounds__(SSFFT_THREADS)
+    krylov_epilogue_kernel(const SlotDev<T> *__restrict__ tab, SlotList list, long long V) {
+  __shared__ double red[32];
+  __shared__ __align__(16) unsigned char sdesc[sizeof(SlotDev<T>)];
+  const int per = vec_items(V);
+  const int n_items = list_items(list, per);
+  int staged = -1;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int k = item / per;
+    const int local = item - k * per;
+    const SlotDev<T> &S = stage_slot<T>(tab, list.ids[k], sdesc, staged);
+    if (slot_done(S.st)) continue;
+    const KRoles<T> kr = kroles<T>(S, S.st->itn);
+    const T c1 = (T)S.st->c_r1;
+    const long long v0 = (long long)local * VEC_CHUNK;
+    const long long v1 = min(V, v0 + VEC_CHUNK);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
+      T pt[6], r1[6], r2[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        pt[c] = kr.Y[c * V + v];
+        r1[c] = kr.P[c * V + v];
+        r2[c] = kr.Q[c * V + v];
+      }
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        const T y = pt[c] - c1 * r1[c];
+        kr.Y[c * V + v] = y;
+        a0 += (double)r2[c] * (double)y;
+        a1 += (double)y * (double)y;
+        a2 += (double)r2[c] * (double)r2[c];
+      }
+    }
+    finish_inverse<T, EPI_MINRES>(S, a0, a1, a2, local, per, red);
   }
 }
 

@@ -418,7 +418,7 @@ template <typename T, typename TF, int PT> static int plane_attrs(int m) {
   CKR(smem_attr(yzinv_kernel<T, TF, EPI_REPROJECT, PT>, m));
   if (sizeof(T) == sizeof(TF)) {
     CKR(smem_attr(zyfwd_kernel<T, T, PRO_TAU, PT>, m));
-    CKR(smem_attr(yzinv_kernel<T, T, EPI_MINRES, PT>, m));
+    CKR(smem_attr(yzinv_kernel<T, T, EPI_PTAU, PT>, m));
   }
   return 0;
 }
@@ -432,7 +432,7 @@ template <typename T, typename TF, int PT> static int cluster_attrs(int m) {
   CKR(smem_attr(yzinv_cl_kernel<T, TF, EPI_REPROJECT, PT>, m));
   if (sizeof(T) == sizeof(TF)) {
     CKR(smem_attr(zyfwd_cl_kernel<T, T, PRO_TAU, PT>, m));
-    CKR(smem_attr(yzinv_cl_kernel<T, T, EPI_MINRES, PT>, m));
+    CKR(smem_attr(yzinv_cl_kernel<T, T, EPI_PTAU, PT>, m));
   }
   return 0;
 }
@@ -459,7 +459,7 @@ template <typename T, typename TF> static int set_kernel_attrs(size_t smax) {
   if (sizeof(T) == sizeof(TF)) {
     CKR(smem_attr(constitutive_kernel<T>, (int)constitutive_smem_bytes()));
     CKR(smem_attr(zfwd_kernel<T, T, PRO_TAU>, m));
-    CKR(smem_attr(zinv_kernel<T, T, EPI_MINRES>, m));
+    CKR(smem_attr(zinv_kernel<T, T, EPI_PTAU>, m));
   }
   return 0;
 }
@@ -919,7 +919,8 @@ static int launch_projector(const LaunchCtx &c, const SlotDev<TF> *tab, ExtIO<TF
 // One MINRES iteration on every listed slot whose solve is not done: the projector passes
 // with the pending vector update in the forward prologue and the scalar recurrence in the
 // inverse epilogue.
-// ev (optional, 8 events): ev[7] before the update kernel, ev[0..5] by the projector.
+// ev (optional, 8 events): ev[7] before the update kernel, ev[0..5] by the projector (the
+// epilogue kernel follows ev[5]).
 template <typename T>
 static int launch_krylov_iteration(const LaunchCtx &c, const SlotDev<T> *tab, bool voxel,
                                    cudaEvent_t *ev = nullptr) {
@@ -934,7 +935,12 @@ static int launch_krylov_iteration(const LaunchCtx &c, const SlotDev<T> *tab, bo
   }
   if (c.launches) *c.launches += 1;
   CK(cudaGetLastError());
-  return launch_projector<T, T, PRO_TAU, EPI_MINRES>(c, tab, {}, ev);
+  CKR((launch_projector<T, T, PRO_TAU, EPI_PTAU>(c, tab, {}, ev)));
+  auto ke = krylov_epilogue_kernel<T>;
+  ke<<<persistent_grid(ke, SSFFT_THREADS, 0, it, c.p->dev), SSFFT_THREADS, 0, c.stream>>>(tab, c.list, c.p->V);
+  if (c.launches) *c.launches += 1;
+  CK(cudaGetLastError());
+  return 0;
 }
 
 // b = P(Sbar - sigma) into each slot's b, max|b| into results[40].  The transform always

@@ -159,7 +159,9 @@ enum { PRO_INPUT = 0, PRO_RESIDUAL = 1, PRO_TANGENT_TABLE = 2, PRO_TANGENT_VOXEL
 //   EPI_RESIDUAL       b = result, max|b|                    (:141-144)
 //   EPI_MINRES         y' and the MINRES recurrence          (krylov.cuh)
 //   EPI_REPROJECT      x = result; strain += x; fluctuation += x   (:154-155)
-enum { EPI_STORE = 0, EPI_RESIDUAL = 1, EPI_MINRES = 2, EPI_REPROJECT = 3 };
+//   EPI_PTAU           y' buffer = P tau (the epilogue kernel, krylov.cuh, forms y' there)
+enum { EPI_STORE = 0, EPI_RESIDUAL = 1, EPI_MINRES = 2, EPI_REPROJECT = 3, EPI_PTAU = 4 };
+#define EPI_SKIPS_DONE(E) ((E) == EPI_MINRES || (E) == EPI_PTAU)
 
 // Stopping tests of scipy's minres after the solution update (last item of the forward
 // pass that applied it, with x2 = |x|^2).
@@ -418,6 +420,8 @@ __device__ __forceinline__ void epilogue_point(const SlotDev<TF> &S, const ExtIO
       kr.X[i] = x;
       S.eps[i] += x;
       S.dfl[i] += x;
+    } else if constexpr (EPI == EPI_PTAU) {
+      kr.Y[i] = (TF)r[q];
     } else {
       const T y = r[q] - c1 * (T)r1v[q];
       kr.Y[i] = (TF)y;
@@ -711,7 +715,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
     const int k = udiv(item, g.fd_it_z);
     const int local = item - k * per;
     const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc, staged);
-    if (EPI == EPI_MINRES && slot_done(S.st)) continue;
+    if (EPI_SKIPS_DONE(EPI) && slot_done(S.st)) continue;
     const long long line0 = (long long)local * g.lz;
     const int nl = (int)min((long long)g.lz, nlines_all - line0);
     const int ti = (nl == g.lz) ? 0 : 1;
@@ -721,6 +725,8 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
     if constexpr (EPI == EPI_MINRES) {
       kr = kroles<TF>(S, S.st->itn);
       c1 = (T)S.st->c_r1;
+    } else if constexpr (EPI == EPI_PTAU) {
+      kr = kroles<TF>(S, S.st->itn);
     } else if constexpr (EPI == EPI_REPROJECT) {
       kr = kroles<TF>(S, 0);
     }
@@ -873,6 +879,8 @@ __device__ __forceinline__ void plane_epilogue(const SlotDev<TF> &S, const ExtIO
   if constexpr (EPI == EPI_MINRES) {
     kr = kroles<TF>(S, S.st->itn);
     c1 = (T)S.st->c_r1;
+  } else if constexpr (EPI == EPI_PTAU) {
+    kr = kroles<TF>(S, S.st->itn);
   } else if constexpr (EPI == EPI_REPROJECT) {
     kr = kroles<TF>(S, 0);
   }
@@ -994,7 +1002,7 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     const int k = udiv(item, g.fd_it_plane);
     const int local = item - k * per;
     const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc, staged);
-    if (EPI == EPI_MINRES && slot_done(S.st)) continue;
+    if (EPI_SKIPS_DONE(EPI) && slot_done(S.st)) continue;
     const int x = udiv(local, g.fd_3);
     const int p = local - 3 * x;
     const cplx<T> *spec = reinterpret_cast<const cplx<T> *>(S.spec);
@@ -1165,7 +1173,7 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     const int k = udiv(item, g.fd_it_plane);
     const int local = item - k * per;
     const SlotDev<TF> &S = stage_slot<TF>(tab, list.ids[k], sdesc, staged);
-    const bool skip = (EPI == EPI_MINRES) && slot_done(S.st);
+    const bool skip = EPI_SKIPS_DONE(EPI) && slot_done(S.st);
     const int x = udiv(local, g.fd_3);
     const int p = local - 3 * x;
     if (!skip) {

@@ -925,7 +925,8 @@ template <typename T> static int profile_impl(ssfft_handle *h, int reps, double 
     CK(cudaEventRecord(h->pev[6], h->stream));
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(h->pev[6]));
-    // pev[7]: before the update kernel; pev[0..5]: the projector's pass slots
+    // pev[7]: before the update kernel; pev[0..5]: the projector's pass slots; pev[6]:
+    // after the epilogue kernel
     for (int i = 0; i < 5; ++i) {
       float ms = 0.f;
       CK(cudaEventElapsedTime(&ms, h->pev[i], h->pev[i + 1]));
@@ -934,11 +935,12 @@ template <typename T> static int profile_impl(ssfft_handle *h, int reps, double 
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, h->pev[7], h->pev[0]));
     acc[5] += ms * 1e-3;
+    CK(cudaEventElapsedTime(&ms, h->pev[5], h->pev[6]));
+    acc[6] += ms * 1e-3;
     CK(cudaEventElapsedTime(&ms, h->pev[7], h->pev[6]));
     acc[7] += ms * 1e-3;
   }
   for (int i = 0; i < 8; ++i) sec[i] = acc[i] / reps;
-  sec[6] = 0.0;
   // every timed iteration must have done its work: a state that stopped (a zero or
   // exactly solved residual) would time kernels that skip their items
   CK(cudaMemcpyAsync(h->h_st, h->sb.st, sizeof(MinresState), cudaMemcpyDeviceToHost, h->stream));
