@@ -157,11 +157,12 @@ enum { PRO_INPUT = 0, PRO_RESIDUAL = 1, PRO_TANGENT_TABLE = 2, PRO_TANGENT_VOXEL
 // ---- epilogue modes of the inverse passes -----------------------------------------------
 //   EPI_STORE          caller's planes = result
 //   EPI_RESIDUAL       b = result, max|b|                    (:141-144)
-//   EPI_MINRES         y' and the MINRES recurrence          (krylov.cuh)
+//   EPI_MINRES         the MINRES dot products' reduction (the epilogue kernel, krylov.cuh;
+//                      not a transform-pass mode)
 //   EPI_REPROJECT      x = result; strain += x; fluctuation += x   (:154-155)
 //   EPI_PTAU           y' buffer = P tau (the epilogue kernel, krylov.cuh, forms y' there)
 enum { EPI_STORE = 0, EPI_RESIDUAL = 1, EPI_MINRES = 2, EPI_REPROJECT = 3, EPI_PTAU = 4 };
-#define EPI_SKIPS_DONE(E) ((E) == EPI_MINRES || (E) == EPI_PTAU)
+#define EPI_SKIPS_DONE(E) ((E) == EPI_PTAU)
 
 // Stopping tests of scipy's minres after the solution update (last item of the forward
 // pass that applied it, with x2 = |x|^2).
@@ -400,13 +401,12 @@ template <typename TF, int PRO> __device__ __forceinline__ bool skip_item(const 
 }
 
 // Per-point epilogue of the inverse passes: r[] is the transformed value of the owned
-// components c0 .. c0 + NC - 1 at point v; accumulates the slot's reduction terms.
+// components c0 .. c0 + NC - 1 at point v; acc0 accumulates the residual's max |b|.
 template <typename T, typename TF, int EPI, int NC>
 __device__ __forceinline__ void epilogue_point(const SlotDev<TF> &S, const ExtIO<TF> &io,
-                                               const KRoles<TF> &kr, T c1, long long V,
-                                               long long v, int c0, const T *r, const TF *r1v,
-                                               const TF *r2v, double &acc0, double &acc1,
-                                               double &acc2) {
+                                               const KRoles<TF> &kr, long long V, long long v,
+                                               int c0, const T *r, double &acc0) {
+  static_assert(EPI != EPI_MINRES, "the MINRES epilogue is the epilogue kernel (krylov.cuh)");
 #pragma unroll
   for (int q = 0; q < NC; ++q) {
     const long long i = (long long)(c0 + q) * V + v;
@@ -420,14 +420,8 @@ __device__ __forceinline__ void epilogue_point(const SlotDev<TF> &S, const ExtIO
       kr.X[i] = x;
       S.eps[i] += x;
       S.dfl[i] += x;
-    } else if constexpr (EPI == EPI_PTAU) {
+    } else {  // EPI_PTAU
       kr.Y[i] = (TF)r[q];
-    } else {
-      const T y = r[q] - c1 * (T)r1v[q];
-      kr.Y[i] = (TF)y;
-      acc0 += (double)r2v[q] * (double)y;
-      acc1 += (double)y * (double)y;
-      acc2 += (double)r2v[q] * (double)r2v[q];
     }
   }
 }
@@ -692,8 +686,6 @@ __global__ void __launch_bounds__(XPASS_THREADS)
   }
 }
 
-#define ZINV_PREFETCH 3  // epilogue elements per thread whose r1/r2 are loaded early
-#define EPI_BATCH 4      // plane epilogue: elements per thread whose loads go out together
 
 template <typename T, typename TF, int EPI>
 __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
@@ -721,32 +713,10 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
     const int ti = (nl == g.lz) ? 0 : 1;
     const int nel = nl * nz;
     KRoles<TF> kr{};
-    T c1 = 0;
-    if constexpr (EPI == EPI_MINRES) {
-      kr = kroles<TF>(S, S.st->itn);
-      c1 = (T)S.st->c_r1;
-    } else if constexpr (EPI == EPI_PTAU) {
+    if constexpr (EPI == EPI_PTAU) {
       kr = kroles<TF>(S, S.st->itn);
     } else if constexpr (EPI == EPI_REPROJECT) {
       kr = kroles<TF>(S, 0);
-    }
-    // MINRES: issue the loads of r1 and r2 for this thread's first elements before the
-    // transform so that their latency overlaps it
-    TF p1[EPI == EPI_MINRES ? ZINV_PREFETCH : 1][6], p2[EPI == EPI_MINRES ? ZINV_PREFETCH : 1][6];
-    const bool prefetch = (EPI == EPI_MINRES) && nel <= ZINV_PREFETCH * (int)blockDim.x;
-    if (EPI == EPI_MINRES && prefetch) {
-#pragma unroll
-      for (int i = 0; i < ZINV_PREFETCH; ++i) {
-        const int e = threadIdx.x + i * blockDim.x;
-        if (e < nel) {
-          const long long v = line0 * nz + e;
-#pragma unroll
-          for (int c = 0; c < 6; ++c) {
-            p1[i][c] = kr.P[c * V + v];
-            p2[i][c] = kr.Q[c * V + v];
-          }
-        }
-      }
     }
     const cplx<T> *spec = reinterpret_cast<const cplx<T> *>(S.spec);
     const int hs = g.hs, nlhs = nl * hs;
@@ -788,7 +758,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
     const LineLayout L(3 * nl, 3 * nl, 0, nz, 1, g.fd_z3[ti], g.fd_z3[ti]);
     cplx<T> *res = smem_fft<T, true, false, true>(bufA, bufB, L, g.pz, tw);
     double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-    auto finish = [&](int e, const TF *r1v, const TF *r2v) {
+    for (int e = threadIdx.x; e < nel; e += blockDim.x) {
       const long long v = line0 * nz + e;
       T r[6];
 #pragma unroll
@@ -797,27 +767,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
         r[2 * p] = Z.x;
         r[2 * p + 1] = Z.y;
       }
-      epilogue_point<T, TF, EPI, 6>(S, io, kr, c1, V, v, 0, r, r1v, r2v, acc0, acc1, acc2);
-    };
-    if (EPI == EPI_MINRES && prefetch) {
-#pragma unroll
-      for (int i = 0; i < ZINV_PREFETCH; ++i) {
-        const int e = threadIdx.x + i * blockDim.x;
-        if (e < nel) finish(e, p1[i], p2[i]);
-      }
-    } else {
-      for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-        TF q1[6], q2[6];
-        if (EPI == EPI_MINRES) {
-          const long long v = line0 * nz + e;
-#pragma unroll
-          for (int c = 0; c < 6; ++c) {
-            q1[c] = kr.P[c * V + v];
-            q2[c] = kr.Q[c * V + v];
-          }
-        }
-        finish(e, q1, q2);
-      }
+      epilogue_point<T, TF, EPI, 6>(S, io, kr, V, v, 0, r, acc0);
     }
     finish_inverse<TF, EPI>(S, acc0, acc1, acc2, local, per, red);
   }
@@ -867,63 +817,22 @@ __device__ __forceinline__ void plane_prologue(const SlotDev<TF> &S, const ExtIO
 }
 
 // Epilogue of a plane item: fin holds components 2p (real part) and 2p + 1 (imaginary
-// part) of the points vbase .. vbase + nel - 1 in padded z lines; accumulates the slot's
-// reduction terms.
+// part) of the points vbase .. vbase + nel - 1 in padded z lines; acc0 accumulates the
+// residual's max |b|.
 template <typename T, typename TF, int EPI>
 __device__ __forceinline__ void plane_epilogue(const SlotDev<TF> &S, const ExtIO<TF> &io,
                                                long long V, long long vbase, int nel, int p,
-                                               const cplx<T> *fin, double &acc0, double &acc1,
-                                               double &acc2) {
+                                               const cplx<T> *fin, double &acc0) {
   KRoles<TF> kr{};
-  T c1 = 0;
-  if constexpr (EPI == EPI_MINRES) {
-    kr = kroles<TF>(S, S.st->itn);
-    c1 = (T)S.st->c_r1;
-  } else if constexpr (EPI == EPI_PTAU) {
+  if constexpr (EPI == EPI_PTAU) {
     kr = kroles<TF>(S, S.st->itn);
   } else if constexpr (EPI == EPI_REPROJECT) {
     kr = kroles<TF>(S, 0);
   }
-  if constexpr (EPI == EPI_MINRES) {
-    // batches of EPI_BATCH elements per thread: all r1 / r2 loads before the y' stores
-    constexpr int B = EPI_BATCH;
-    const long long o0 = (2 * p) * V, o1 = (2 * p + 1) * V;
-    for (int e0 = threadIdx.x; e0 < nel; e0 += B * blockDim.x) {
-      T l0[B], l1[B], m0[B], m1[B];
-#pragma unroll
-      for (int b = 0; b < B; ++b) {
-        const int e = e0 + b * blockDim.x;
-        if (e < nel) {
-          const long long v = vbase + e;
-          l0[b] = (T)kr.P[o0 + v];
-          l1[b] = (T)kr.P[o1 + v];
-          m0[b] = (T)kr.Q[o0 + v];
-          m1[b] = (T)kr.Q[o1 + v];
-        }
-      }
-#pragma unroll
-      for (int b = 0; b < B; ++b) {
-        const int e = e0 + b * blockDim.x;
-        if (e < nel) {
-          const long long v = vbase + e;
-          const cplx<T> Z = fin[sidx<true>(e)];
-          const T y0 = Z.x - c1 * l0[b];
-          const T y1 = Z.y - c1 * l1[b];
-          kr.Y[o0 + v] = (TF)y0;
-          kr.Y[o1 + v] = (TF)y1;
-          acc0 += (double)m0[b] * (double)y0 + (double)m1[b] * (double)y1;
-          acc1 += (double)y0 * (double)y0 + (double)y1 * (double)y1;
-          acc2 += (double)m0[b] * (double)m0[b] + (double)m1[b] * (double)m1[b];
-        }
-      }
-    }
-  } else {
-    for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-      const cplx<T> Z = fin[sidx<true>(e)];
-      const T r[2] = {Z.x, Z.y};
-      epilogue_point<T, TF, EPI, 2>(S, io, kr, c1, V, vbase + e, 2 * p, r, nullptr, nullptr,
-                                    acc0, acc1, acc2);
-    }
+  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+    const cplx<T> Z = fin[sidx<true>(e)];
+    const T r[2] = {Z.x, Z.y};
+    epilogue_point<T, TF, EPI, 2>(S, io, kr, V, vbase + e, 2 * p, r, acc0);
   }
 }
 
@@ -1030,7 +939,7 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     const LineLayout Lz(ny, ny, 0, nz, 1, g.fd_ny, g.fd_ny);
     cplx<T> *fin = smem_fft<T, true, false, true>(oth, res, Lz, g.pz, twz);
     double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-    plane_epilogue<T, TF, EPI>(S, io, V, (long long)x * ny * nz, ny * nz, p, fin, acc0, acc1, acc2);
+    plane_epilogue<T, TF, EPI>(S, io, V, (long long)x * ny * nz, ny * nz, p, fin, acc0);
     finish_inverse<TF, EPI>(S, acc0, acc1, acc2, local, per, red);
   }
 }
@@ -1217,8 +1126,7 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
       const LineLayout Lz(R, R, 0, nz, 1, cq.fd_R, cq.fd_R);
       cplx<T> *fin = smem_fft<T, true, false, true>(res, oth, Lz, g.pz, twz);
       double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-      plane_epilogue<T, TF, EPI>(S, io, V, ((long long)x * ny + y0) * nz, R * nz, p, fin, acc0,
-                                 acc1, acc2);
+      plane_epilogue<T, TF, EPI>(S, io, V, ((long long)x * ny + y0) * nz, R * nz, p, fin, acc0);
       finish_inverse<TF, EPI>(S, acc0, acc1, acc2, local * C + rank, per * C, red);
     }
   }
