@@ -108,35 +108,6 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
   }
 }
 
-// Points per item of the streaming Krylov kernels (update and epilogue).  Each item first
-// asks L2 for all of its input streams (stream_prefetch), so with every block's current
-// item in flight the prefetched bytes (about 1024 x 124 B a block in the update kernel)
-// stay far below the 126 MB L2.
-#define STREAM_CHUNK 1024
-
-__host__ __device__ inline int stream_items(long long V) {
-  return (int)((V + STREAM_CHUNK - 1) / STREAM_CHUNK);
-}
-
-// Prefetch into L2 the elements [v0, v1) of `planes` component planes of V elements each
-// (plane c at base + c V), one bulk prefetch per plane issued by the first threads of the
-// block.  Only whole 16-byte-aligned chunks inside each plane are requested; the ragged ends
-// are left to the ordinary loads, so nothing outside the arrays is touched.  The loads that
-// follow then find their lines in L2 or in flight there: DRAM sees a whole item's requests
-// at once, without registers holding them.
-template <typename T>
-__device__ __forceinline__ void stream_prefetch(const T *base, int planes, long long V,
-                                                long long v0, long long v1) {
-  for (int c = threadIdx.x; c < planes; c += blockDim.x) {
-    const uintptr_t a = (uintptr_t)(base + c * V + v0), e = (uintptr_t)(base + c * V + v1);
-    const uintptr_t a16 = (a + 15) & ~(uintptr_t)15, e16 = e & ~(uintptr_t)15;
-    if (e16 > a16)
-      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a16),
-                   "r"((unsigned)(e16 - a16))
-                   : "memory");
-  }
-}
-
 // The forward half of a Krylov matvec, elementwise: for every listed slot whose solve is
 // not done, the pending update of the previous iteration (u_j = y' - coef u_{j-1}, w, x,
 // |x|^2 and, in the slot's last item, the stopping tests) and tau = K (s u_j), which
@@ -149,7 +120,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     krylov_update_kernel(const SlotDev<T> *__restrict__ tab, SlotList list, long long V) {
   __shared__ double red[32];
   __shared__ __align__(16) unsigned char sdesc[sizeof(SlotDev<T>)];
-  const int per = stream_items(V);
+  const int per = vec_items(V);
   const int n_items = list_items(list, per);
   int staged = -1;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
@@ -158,19 +129,8 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     const SlotDev<T> &S = stage_slot<T>(tab, list.ids[k], sdesc, staged);
     if (slot_done(S.st)) continue;
     const KrylovIn<T, T> u = krylov_in<T, T>(S);
-    const long long v0 = (long long)local * STREAM_CHUNK;
-    const long long v1 = min(V, v0 + STREAM_CHUNK);
-    stream_prefetch(u.r.P, 6, V, v0, v1);
-    if (u.on) {
-      stream_prefetch(u.r.Y, 6, V, v0, v1);
-      stream_prefetch(u.r.W1, 6, V, v0, v1);
-      stream_prefetch(u.r.W2, 6, V, v0, v1);
-      stream_prefetch(u.r.X, 6, V, v0, v1);
-    }
-    if constexpr (PRO == PRO_TANGENT_TABLE)
-      stream_prefetch(S.gid, 1, V, v0, v1);
-    else
-      stream_prefetch(S.kvox, 21, V, v0, v1);
+    const long long v0 = (long long)local * VEC_CHUNK;
+    const long long v1 = min(V, v0 + VEC_CHUNK);
     T *tau_out = u.r.Y;
     double xx = 0.0;
     for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
@@ -192,7 +152,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     krylov_epilogue_kernel(const SlotDev<T> *__restrict__ tab, SlotList list, long long V) {
   __shared__ double red[32];
   __shared__ __align__(16) unsigned char sdesc[sizeof(SlotDev<T>)];
-  const int per = stream_items(V);
+  const int per = vec_items(V);
   const int n_items = list_items(list, per);
   int staged = -1;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
@@ -202,11 +162,8 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     if (slot_done(S.st)) continue;
     const KRoles<T> kr = kroles<T>(S, S.st->itn);
     const T c1 = (T)S.st->c_r1;
-    const long long v0 = (long long)local * STREAM_CHUNK;
-    const long long v1 = min(V, v0 + STREAM_CHUNK);
-    stream_prefetch(kr.Y, 6, V, v0, v1);
-    stream_prefetch(kr.P, 6, V, v0, v1);
-    stream_prefetch(kr.Q, 6, V, v0, v1);
+    const long long v0 = (long long)local * VEC_CHUNK;
+    const long long v1 = min(V, v0 + VEC_CHUNK);
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
       T pt[6], r1[6], r2[6];

@@ -391,9 +391,7 @@ static int plan_create(GridPlan &p, const ssfft_config *cfg, cudaStream_t stream
   need = std::max(need, (size_t)NORM_VALS * norm_items(p.V));
   need = std::max(need, (size_t)21 * vec_items(p.V));
   need = std::max(need, (size_t)vec_items(6 * p.V));
-  need = std::max(need, (size_t)3 * stream_items(p.V));  // update and epilogue kernels
   if (items_z(g) > MAX_ITEMS_PER_SLOT || vec_items(6 * p.V) > MAX_ITEMS_PER_SLOT ||
-      stream_items(p.V) > MAX_ITEMS_PER_SLOT ||
       items_y(g) > (1 << 30) / 2)
     return ssfft_internal_fail(SSFFT_E_UNSUPPORTED, "grid too large for the reduction partials");
   p.partial_doubles = need;
@@ -927,7 +925,7 @@ template <typename T>
 static int launch_krylov_iteration(const LaunchCtx &c, const SlotDev<T> *tab, bool voxel,
                                    cudaEvent_t *ev = nullptr) {
   if (ev) cudaEventRecord(ev[7], c.stream);
-  const long long it = (long long)c.cap * stream_items(c.p->V);
+  const long long it = (long long)c.cap * vec_items(c.p->V);
   if (voxel) {
     auto k = krylov_update_kernel<T, PRO_TANGENT_VOXEL>;
     k<<<persistent_grid(k, SSFFT_THREADS, 0, it, c.p->dev), SSFFT_THREADS, 0, c.stream>>>(tab, c.list, c.p->V);
