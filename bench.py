@@ -717,10 +717,13 @@ def accuracy_mode(args, w):
     print(json.dumps(out), flush=True)
 
 
-# DRAM read + write bytes of one steady-state zfwd launch on plain128, from an ncu
-# --set full capture of `--mode kernels --workload plain128`: 260.4 MB read + 168.9 MB
-# written (algorithmic 462 MB).
-ZFWD_PLAIN128_TRAFFIC_BYTES = 429.4e6
+# DRAM read + write bytes of one steady-state launch of each Krylov kernel on plain128
+# (128^3, mixed precision, three-pass cluster path), from one-launch ncu captures of
+# `--mode kernels --workload plain128` (profiles/krylov_kernels_plain128.md).  The update
+# kernel reads 260.1 MB and writes 154.2 MB against 461 MB algorithmic: part of its writes
+# are still in L2 when it ends.
+PLAIN128_TRAFFIC_BYTES = {"update": 414.4e6, "epilogue": 174.8e6, "zfwd": 56.6e6,
+                          "xpass": 52.6e6, "zinv": 58.9e6}
 
 
 def plain128_roofline(device):
@@ -741,7 +744,7 @@ def plain128_roofline(device):
     achieved = bpv[dom] * V / per_kernel[dom] / 1e9
     return {"bound": "hbm", "workload": "plain128 Krylov iteration", "kernel": dom,
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": ZFWD_PLAIN128_TRAFFIC_BYTES if dom == "zfwd" else None,
+            "traffic": PLAIN128_TRAFFIC_BYTES.get(dom),
             "traffic_unit": "bytes per launch (ncu capture)",
             "algorithmic_bytes": bpv[dom] * V, "peak_kind": kind,
             "per_kernel_us": {k: v * 1e6 for k, v in per_kernel.items()},
@@ -883,8 +886,8 @@ def main():
             "gpu_launches": int(launches1 - launches0),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": (ZFWD_PLAIN128_TRAFFIC_BYTES
-                                     if args.workload == "plain128" and dom == "zfwd" else None),
+                         "traffic": (PLAIN128_TRAFFIC_BYTES.get(dom)
+                                     if args.workload == "plain128" else None),
                          "peak_kind": peak_kind,
                          "per_kernel_us": {k: v * 1e6 for k, v in per_kernel.items()},
                          "krylov_iteration_us": prof[7] * 1e6,
