@@ -532,7 +532,11 @@ def serve_mode(args, w):
                                                       "stream, one at a time",
                                           "solves_per_s": plain_value,
                                           "served_solves_per_s_same_requests": served_sub},
+            # the same requests both ways; the served side is all of them at once, so its
+            # makespan ends with the longest request (a tail the one-at-a-time sum has not)
             "served_over_plain": served_sub / plain_value,
+            # the stream's steady served rate over the plain rate of the same prefix's mix
+            "served_stream_over_plain": value / plain_value,
             "stress_rel_l2_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs)),
                                             "requests": len(errs)},
             "cpu_class_on_gpu": cpu_gpu,
