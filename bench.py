@@ -53,6 +53,9 @@ WORKLOADS = {
     # elastic x10 with probability 1/2, uniaxial x 1e-3 to 1% strain in 50 steps.
     "twophase256": dict(n=256, grains=2000, steps=50, dt=0.2, rate=1e-3, gtol=1e-6,
                         ltol=1e-5, precision="mixed", seed=0, model="twophase"),
+    # its 128^3 analog: the same physics and grain size (250 grains), eight times cheaper
+    "twophase128": dict(n=128, grains=250, steps=50, dt=0.2, rate=1e-3, gtol=1e-6,
+                        ltol=1e-5, precision="mixed", seed=0, model="twophase"),
     # Serving stream: requests with N ~ U{32,48,64,96}, 20-400 periodic Voronoi grains,
     # elastic or FCC EVP (p = 1/2), uniaxial or biaxial strain rate 1e-3, 10-50 steps,
     # Poisson arrivals at 50 req/s; the first `count` requests of the seeded stream.
@@ -704,20 +707,28 @@ def accuracy_mode(args, w):
         h = make_handle(w, rot, ids, 0, precision=prec)
         st = SolveStats()
         h.timer_start()
-        res, _ = run_solve(h, w, st)
+        failure = None
+        try:
+            res, _ = run_solve(h, w, st)
+        except ValueError as e:  # the reference's own failure: min time increment reached
+            failure, res = str(e), None
         t = h.timer_stop()
-        stress[prec] = res["stress"]
+        reached = sum(a[1] for a in st.attempts if a[2])
         out[prec] = {"device_s": t, "steps": st.steps, "cutbacks": getattr(st, "cutbacks", None),
                      "newton": int(sum(st.newton_iterations)),
-                     "krylov": int(sum(st.krylov_iterations)),
-                     "mean_stress_xx": float(res["stress"][:, 0].mean())}
+                     "krylov": int(sum(st.krylov_iterations)), "time_reached": reached,
+                     "end_time": w["steps"] * w["dt"], "failure": failure}
+        if res is not None:
+            stress[prec] = res["stress"]
+            out[prec]["mean_stress_xx"] = float(res["stress"][:, 0].mean())
         h.close()
         print(json.dumps({prec: out[prec]}), flush=True)
         # per attempted increment: t, dt, converged, Newton, Krylov, eq. error, max
         # constitutive iterations (where the two precisions part ways)
         print(json.dumps({prec + "_attempts": st.attempts}), flush=True)
-    a, b = stress["mixed"], stress["fp64"]
-    out["stress_rel_l2_mixed_vs_fp64"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    if "mixed" in stress and "fp64" in stress:
+        a, b = stress["mixed"], stress["fp64"]
+        out["stress_rel_l2_mixed_vs_fp64"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
     print(json.dumps(out), flush=True)
 
 

@@ -63,6 +63,86 @@ template <typename T> __device__ __forceinline__ void cp_async_scalar(T *dst, co
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// ---- bulk copies (the TMA engine, without a tensor map) ------------------------------
+// cp.async.bulk moves a contiguous run of 16-byte multiples from global to this block's
+// shared memory and signals an mbarrier when the bytes have landed: one instruction per
+// run instead of one per element.  The destination is the issuing block's own shared
+// memory; nothing here multicasts.  A block owns one barrier for its tile loads and flips
+// the parity it waits for after each use.
+
+// Set when a bounded mbarrier wait gives up (the copy never completed); nothing clears it.
+// One per translation unit (internal linkage).
+static __device__ int g_bulk_wait_timeouts;
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+// One thread initialises the barrier (expected arrivals: one, the issuing thread's
+// arrive.expect_tx); the block syncs before any use.
+__device__ __forceinline__ void bulk_barrier_init(uint64_t *bar) {
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+}
+
+// Wait for the barrier phase with the given parity, at most about 2^22 polls (each poll may
+// suspend the thread for a while); on giving up, flag it and go on rather than hang.
+__device__ __forceinline__ void bulk_barrier_wait(uint64_t *bar, unsigned parity) {
+  for (int i = 0; i < (1 << 22); ++i) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return;
+  }
+  atomicExch(&g_bulk_wait_timeouts, 1);
+}
+
+// Block-cooperative copy of n_outer x n_inner runs of `bytes` bytes each, run (o, i) from
+// src + o * s_outer + i * s_inner bytes to dst + o * d_outer + i * d_inner bytes, completing
+// on `bar` (the caller then waits on it with its current parity).  Returns false, having
+// issued nothing, unless every address, size and step is a multiple of 16 bytes; the caller
+// then copies another way.  The answer is the same in every thread.  Call after a block
+// barrier that ends all reads of the destination.
+__device__ __forceinline__ bool bulk_copy_rows(void *dst, const void *src, int n_outer,
+                                               int n_inner, unsigned bytes, long long d_outer,
+                                               long long d_inner, long long s_outer,
+                                               long long s_inner, uint64_t *bar) {
+  const int rows = n_outer * n_inner;
+  const bool ok = rows > 0 && bytes > 0 && (bytes & 15u) == 0 &&
+                  ((uintptr_t)dst & 15u) == 0 && ((uintptr_t)src & 15u) == 0 &&
+                  ((d_outer | d_inner | s_outer | s_inner) & 15) == 0;
+  if (!ok) return false;
+  if (threadIdx.x < 32) {
+    if (threadIdx.x == 0) {
+      // order this block's earlier generic-proxy accesses of the destination before the
+      // asynchronous writes, then announce the bytes to expect
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+                   "r"((unsigned)(bytes * (unsigned)rows))
+                   : "memory");
+    }
+    __syncwarp();
+    for (int r = threadIdx.x; r < rows; r += 32) {
+      const int o = r / n_inner, i = r - o * n_inner;
+      const char *s = (const char *)src + o * s_outer + i * s_inner;
+      char *d = (char *)dst + o * d_outer + i * d_inner;
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+              smem_u32(d)),
+          "l"(s), "r"(bytes), "r"(smem_u32(bar))
+          : "memory");
+    }
+  }
+  return true;
+}
+
 // ---- block reductions (double) ------------------------------------------------------
 
 __device__ __forceinline__ double warp_sum(double v) {

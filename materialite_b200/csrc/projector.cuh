@@ -553,7 +553,10 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *bufB = bufA + g.ky * ny;
   cplx<T> *tw = bufB + g.ky * ny;
+  __shared__ __align__(8) uint64_t tile_bar;
   load_table<T>(tw, g.twy, ny);
+  bulk_barrier_init(&tile_bar);
+  unsigned tile_phase = 0;
   const int per = items_y(g);
   const int n_items = list_items(list, per);
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
@@ -570,11 +573,17 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     const int ti = (nk == g.ky) ? 0 : 1;
     cplx<T> *base = reinterpret_cast<cplx<T> *>(S.spec) + c * g.S + (long long)x * ny * hs + k0;
     __syncthreads();
-    for (int e = threadIdx.x; e < ny * nk; e += blockDim.x) {
-      const int y = udiv(e, g.fd_ky[ti]), kk = e - y * nk;
-      cp_async_elem<T>(&bufA[y * nk + kk], &base[(long long)y * hs + kk]);
+    constexpr long long E = sizeof(cplx<T>);
+    if (bulk_copy_rows(bufA, base, ny, 1, (unsigned)(nk * E), nk * E, 0, hs * E, 0, &tile_bar)) {
+      bulk_barrier_wait(&tile_bar, tile_phase);
+      tile_phase ^= 1;
+    } else {
+      for (int e = threadIdx.x; e < ny * nk; e += blockDim.x) {
+        const int y = udiv(e, g.fd_ky[ti]), kk = e - y * nk;
+        cp_async_elem<T>(&bufA[y * nk + kk], &base[(long long)y * hs + kk]);
+      }
+      cp_async_wait_all();
     }
-    cp_async_wait_all();
     __syncthreads();
     const LineLayout L(nk, nk, 0, 1, nk, g.fd_ky[ti], g.fd_ky[ti]);
     cplx<T> *res = smem_fft<T, INV, true>(bufA, bufB, L, g.py, tw);
@@ -641,7 +650,10 @@ __global__ void __launch_bounds__(XPASS_THREADS)
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *bufB = bufA + 6 * sst;
   cplx<T> *tw = bufB + 6 * sst;
+  __shared__ __align__(8) uint64_t tile_bar;
   load_table<T>(tw, g.twx, nx);
+  bulk_barrier_init(&tile_bar);
+  unsigned tile_phase = 0;
   const int per = items_x(g);
   const int n_items = list_items(list, per);
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
@@ -657,12 +669,20 @@ __global__ void __launch_bounds__(XPASS_THREADS)
     const int slab = nx * nk;                      // live elements per component
     cplx<T> *spec = reinterpret_cast<cplx<T> *>(S.spec);
     __syncthreads();
-    for (int e = threadIdx.x; e < 6 * slab; e += blockDim.x) {
-      const int c = udiv(e, g.fd_xslab[ti]), rem = e - c * slab;
-      const int x = udiv(rem, g.fd_kx[ti]), kk = rem - x * nk;
-      cp_async_elem<T>(&bufA[c * sst + x * nk + kk], &spec[c * g.S + ((long long)x * ny + y) * hs + k0 + kk]);
+    constexpr long long E = sizeof(cplx<T>);
+    // rows (c, x): nk columns each, from spec[c][x][y][k0..]
+    if (bulk_copy_rows(bufA, spec + (long long)y * hs + k0, 6, nx, (unsigned)(nk * E), sst * E,
+                       nk * E, g.S * E, (long long)ny * hs * E, &tile_bar)) {
+      bulk_barrier_wait(&tile_bar, tile_phase);
+      tile_phase ^= 1;
+    } else {
+      for (int e = threadIdx.x; e < 6 * slab; e += blockDim.x) {
+        const int c = udiv(e, g.fd_xslab[ti]), rem = e - c * slab;
+        const int x = udiv(rem, g.fd_kx[ti]), kk = rem - x * nk;
+        cp_async_elem<T>(&bufA[c * sst + x * nk + kk], &spec[c * g.S + ((long long)x * ny + y) * hs + k0 + kk]);
+      }
+      cp_async_wait_all();
     }
-    cp_async_wait_all();
     __syncthreads();
     const LineLayout L(6 * nk, nk, sst, 1, nk, g.fd_x6k[ti], g.fd_kx[ti]);
     cplx<T> *res = smem_fft<T, false, true>(bufA, bufB, L, g.px, tw);
@@ -699,7 +719,10 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
   cplx<T> *bufA = reinterpret_cast<cplx<T> *>(smem_raw);
   cplx<T> *bufB = bufA + zbuf_elems(g.lz, nz);
   cplx<T> *tw = bufB + zbuf_elems(g.lz, nz);
+  __shared__ __align__(8) uint64_t tile_bar;
   load_table<T>(tw, g.twz, nz);
+  bulk_barrier_init(&tile_bar);
+  unsigned tile_phase = 0;
   const int per = items_z(g);
   const int n_items = list_items(list, per);
   int staged = -1;  // slot whose descriptor sdesc holds
@@ -725,11 +748,19 @@ __global__ void __launch_bounds__(SSFFT_THREADS, Z_MIN_BLOCKS(T))
     // are consecutive rows of the spectrum)
     const bool staged_half = 6 * nlhs <= zbuf_elems(g.lz, nz);
     if (staged_half) {
-      for (int e = threadIdx.x; e < 6 * nlhs; e += blockDim.x) {
-        const int c = udiv(e, g.fd_znh[ti]), rem = e - c * nlhs;
-        cp_async_elem<T>(&bufB[e], &spec[c * g.S + line0 * hs + rem]);
+      constexpr long long E = sizeof(cplx<T>);
+      // six bulk copies, one per component, where the runs are 16-byte aligned
+      if (bulk_copy_rows(bufB, spec + line0 * hs, 6, 1, (unsigned)(nlhs * E), nlhs * E, 0,
+                         g.S * E, 0, &tile_bar)) {
+        bulk_barrier_wait(&tile_bar, tile_phase);
+        tile_phase ^= 1;
+      } else {
+        for (int e = threadIdx.x; e < 6 * nlhs; e += blockDim.x) {
+          const int c = udiv(e, g.fd_znh[ti]), rem = e - c * nlhs;
+          cp_async_elem<T>(&bufB[e], &spec[c * g.S + line0 * hs + rem]);
+        }
+        cp_async_wait_all();
       }
-      cp_async_wait_all();
       __syncthreads();
     }
     // rebuild the full z spectrum of Z = A + iB from the stored half (Hermitian in z)
@@ -901,8 +932,11 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
   cplx<T> *bufB = bufA + cap;
   cplx<T> *twy = bufB + cap;
   cplx<T> *twz = twy + ny;
+  __shared__ __align__(8) uint64_t tile_bar;
   load_table<T>(twy, g.twy, ny);
   load_table<T>(twz, g.twz, nz);
+  bulk_barrier_init(&tile_bar);
+  unsigned tile_phase = 0;
   const int per = items_plane(g);
   const int n_items = list_items(list, per);
   const int plane = ny * hs;
@@ -916,11 +950,19 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     const int p = local - 3 * x;
     const cplx<T> *spec = reinterpret_cast<const cplx<T> *>(S.spec);
     __syncthreads();
-    for (int e = threadIdx.x; e < 2 * plane; e += blockDim.x) {
-      const int c = udiv(e, g.fd_plane), rem = e - c * plane;
-      cp_async_elem<T>(&bufA[e], &spec[(2 * p + c) * g.S + (long long)x * plane + rem]);
+    constexpr long long E = sizeof(cplx<T>);
+    // the pair's two half-spectrum planes, one bulk copy each where 16-byte aligned
+    if (bulk_copy_rows(bufA, spec + (2 * p) * g.S + (long long)x * plane, 2, 1,
+                       (unsigned)(plane * E), plane * E, 0, g.S * E, 0, &tile_bar)) {
+      bulk_barrier_wait(&tile_bar, tile_phase);
+      tile_phase ^= 1;
+    } else {
+      for (int e = threadIdx.x; e < 2 * plane; e += blockDim.x) {
+        const int c = udiv(e, g.fd_plane), rem = e - c * plane;
+        cp_async_elem<T>(&bufA[e], &spec[(2 * p + c) * g.S + (long long)x * plane + rem]);
+      }
+      cp_async_wait_all();
     }
-    cp_async_wait_all();
     __syncthreads();
     const LineLayout Ly(2 * hs, hs, plane, 1, hs, g.fd_2hs, g.fd_hs);
     cplx<T> *res = smem_fft<T, true, true>(bufA, bufB, Ly, g.py, twy);
@@ -1065,8 +1107,11 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
   cplx<T> *bufB = bufA + cq.cap;
   cplx<T> *twy = bufB + cq.cap;
   cplx<T> *twz = twy + ny;
+  __shared__ __align__(8) uint64_t tile_bar;
   load_table<T>(twy, g.twy, ny);
   load_table<T>(twz, g.twz, nz);
+  bulk_barrier_init(&tile_bar);
+  unsigned tile_phase = 0;
   // after the y transform the result is in bufA for an even stage count
   cplx<T> *res = (g.py.nrad & 1) ? bufB : bufA;
   cplx<T> *oth = (g.py.nrad & 1) ? bufA : bufB;
@@ -1089,11 +1134,19 @@ __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
       const cplx<T> *spec = reinterpret_cast<const cplx<T> *>(S.spec) + (2 * p + cown) * g.S +
                             (long long)x * plane + k0;
       __syncthreads();
-      for (int e = threadIdx.x; e < ny * Lq; e += blockDim.x) {
-        const int y = udiv(e, cq.fd_Lq), kl = e - y * Lq;
-        cp_async_elem<T>(&bufA[e], &spec[(long long)y * hs + kl]);
+      constexpr long long E = sizeof(cplx<T>);
+      // the block's Lq columns of every row y: one bulk copy per row where 16-byte aligned
+      if (bulk_copy_rows(bufA, spec, ny, 1, (unsigned)(Lq * E), Lq * E, 0, hs * E, 0,
+                         &tile_bar)) {
+        bulk_barrier_wait(&tile_bar, tile_phase);
+        tile_phase ^= 1;
+      } else {
+        for (int e = threadIdx.x; e < ny * Lq; e += blockDim.x) {
+          const int y = udiv(e, cq.fd_Lq), kl = e - y * Lq;
+          cp_async_elem<T>(&bufA[e], &spec[(long long)y * hs + kl]);
+        }
+        cp_async_wait_all();
       }
-      cp_async_wait_all();
       __syncthreads();
       const LineLayout Ly(Lq, Lq, 0, 1, Lq, cq.fd_Lq, cq.fd_Lq);
       smem_fft<T, true, true>(bufA, bufB, Ly, g.py, twy);
