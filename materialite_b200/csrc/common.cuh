@@ -104,18 +104,23 @@ __device__ __forceinline__ void bulk_barrier_wait(uint64_t *bar, unsigned parity
   atomicExch(&g_bulk_wait_timeouts, 1);
 }
 
+#define BULK_MIN_BYTES 1024
+
 // Block-cooperative copy of n_outer x n_inner runs of `bytes` bytes each, run (o, i) from
 // src + o * s_outer + i * s_inner bytes to dst + o * d_outer + i * d_inner bytes, completing
 // on `bar` (the caller then waits on it with its current parity).  Returns false, having
-// issued nothing, unless every address, size and step is a multiple of 16 bytes; the caller
-// then copies another way.  The answer is the same in every thread.  Call after a block
-// barrier that ends all reads of the destination.
+// issued nothing, unless every address, size and step is a multiple of 16 bytes and the runs
+// are at least BULK_MIN_BYTES long; the caller then copies another way.  The answer is the
+// same in every thread.  Call after a block barrier that ends all reads of the destination.
 __device__ __forceinline__ bool bulk_copy_rows(void *dst, const void *src, int n_outer,
                                                int n_inner, unsigned bytes, long long d_outer,
                                                long long d_inner, long long s_outer,
                                                long long s_inner, uint64_t *bar) {
   const int rows = n_outer * n_inner;
-  const bool ok = rows > 0 && bytes > 0 && (bytes & 15u) == 0 &&
+  // runs under BULK_MIN_BYTES cost more as bulk copies issued from one warp than as
+  // per-element cp.async spread over the block (measured: the x pass's 64-byte runs took
+  // twice as long); only long runs go to the bulk engine
+  const bool ok = rows > 0 && bytes >= BULK_MIN_BYTES && (bytes & 15u) == 0 &&
                   ((uintptr_t)dst & 15u) == 0 && ((uintptr_t)src & 15u) == 0 &&
                   ((d_outer | d_inner | s_outer | s_inner) & 15) == 0;
   if (!ok) return false;

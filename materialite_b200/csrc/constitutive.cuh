@@ -40,9 +40,9 @@ struct PhaseParams {
 
 template <typename T> struct ConstArgs {
   long long V;
-  const T *eps;            // 6 planes
-  const T *guess;          // 6 planes
-  T *sig;                  // 6 planes (out)
+  const double *eps;       // 6 planes
+  const double *guess;     // 6 planes
+  double *sig;             // 6 planes (out)
   T *kvox;                 // 21 planes (out, EVP voxels) or null (table mode)
   const T *ktab;           // table-mode tangents [n_gid][21]
   const int32_t *gid;      // table-mode tangent index
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     const PhaseParams &P = a.params[a.phase ? a.phase[v] : 0];
     if (P.kind != PHASE_J2) continue;
     double eps[6], epo[6], s[6], mean, q;
-    load6<T>(a.eps, V, v, eps);
+    load6<double>(a.eps, V, v, eps);
     load6<double>(a.ep_old, V, v, epo);
     j2_predictor(P, eps, epo, s, mean, q);
     const double y_old = a.g_old[v], eq_old = a.Gam_old[v];
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(CONST_THREADS, 3)
     const int ph = a.phase ? a.phase[v] : 0;
     const PhaseParams &P = sp[ph];
     double eps[6];
-    load6<T>(a.eps, V, v, eps);
+    load6<double>(a.eps, V, v, eps);
     if (P.kind == PHASE_ELASTIC) {
       double s[6];
       if (a.kvox) {
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(CONST_THREADS, 3)
         }
       }
 #pragma unroll
-      for (int c = 0; c < 6; ++c) a.sig[c * V + v] = (T)s[c];
+      for (int c = 0; c < 6; ++c) a.sig[c * V + v] = s[c];
       my_iters = max(my_iters, 1);
       continue;
     }
@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(CONST_THREADS, 3)
 #pragma unroll
         for (int c = 0; c < 6; ++c) sig[c] = s[c] + (c < 3 ? mean : 0.0);
 #pragma unroll
-        for (int c = 0; c < 6; ++c) a.sig[c * V + v] = (T)sig[c];
+        for (int c = 0; c < 6; ++c) a.sig[c * V + v] = sig[c];
 #pragma unroll
         for (int i = 0; i < 6; ++i)
 #pragma unroll
@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(CONST_THREADS, 3)
 #pragma unroll
       for (int c = 0; c < 6; ++c) sig[c] = (1.0 - ratio * dp) * s[c] + (c < 3 ? mean : 0.0);
 #pragma unroll
-      for (int c = 0; c < 6; ++c) a.sig[c * V + v] = (T)sig[c];
+      for (int c = 0; c < 6; ++c) a.sig[c * V + v] = sig[c];
       // consistent tangent C - t1 I_dev + t2 s (x) s on plastic points, C on elastic ones
       // (:148-163)
       const double t1 = elastic ? 0.0 : 2.0 * P.shear * ratio * dp;
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(CONST_THREADS, 3)
     // ---------------- crystal elasto-viscoplasticity ----------------
     const double *Rm = a.rm_tab + (long long)a.orient[v] * 36;
     double gs[6];
-    load6<T>(a.guess, V, v, gs);
+    load6<double>(a.guess, V, v, gs);
     double gnorm = 0.0;
 #pragma unroll
     for (int c = 0; c < 6; ++c) gnorm += gs[c] * gs[c];
@@ -579,7 +579,7 @@ __global__ void __launch_bounds__(CONST_THREADS, 3)
       double acc = 0.0;
 #pragma unroll
       for (int j = 0; j < 6; ++j) acc += Rm[j * 6 + i] * sig[j];
-      a.sig[i * V + v] = (T)acc;
+      a.sig[i * V + v] = acc;
     }
     // tangent M^-1 in the crystal frame (columns from the factor), then
     // K_s = Rm^T M^-1 Rm one row at a time

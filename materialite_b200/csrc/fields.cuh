@@ -75,23 +75,22 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
-        T f = S.dfl[c * V + v];
-        if (reset) f = 0;
-        else if (fs != 1.0) f = (T)((double)f * fs);
+        double f = S.dfl[c * V + v];
+        if (reset) f = 0.0;
+        else if (fs != 1.0) f = f * fs;
         if (reset || fs != 1.0) S.dfl[c * V + v] = f;
         // same association as the reference: (old + dEbar + fluct) + correction
-        double e = (double)S.eps_old[c * V + v] + sv.dEbar[c];
-        S.eps[c * V + v] = (T)((e + (double)f) + sv.corr[c]);
+        double e = S.eps_old[c * V + v] + sv.dEbar[c];
+        S.eps[c * V + v] = (e + f) + sv.corr[c];
       }
       if (first) {
         double y[6];
         K.apply(v, sv.dEbar, y);
 #pragma unroll
-        for (int c = 0; c < 6; ++c) S.sig[c * V + v] = (T)(sv.dS[c] + y[c]);
+        for (int c = 0; c < 6; ++c) S.sig[c * V + v] = sv.dS[c] + y[c];
       } else {
 #pragma unroll
-        for (int c = 0; c < 6; ++c)
-          S.sig[c * V + v] = (T)((double)S.sig_old[c * V + v] + sv.dS[c]);
+        for (int c = 0; c < 6; ++c) S.sig[c * V + v] = S.sig_old[c * V + v] + sv.dS[c];
       }
     }
   }
@@ -113,7 +112,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     const long long i0 = (long long)local * VEC_CHUNK;
     const long long i1 = min(n, i0 + VEC_CHUNK);
     for (long long i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
-      const T d = dx[i];
+      const double d = dx[i];
       S.eps[i] += d;
       S.dfl[i] += d;
     }

@@ -161,7 +161,7 @@ __global__ void group_swap_stress_kernel(SlotDev<T> *tab, const int *ids, const 
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   for (int k = 0; k < counts[GL_NEWTON]; ++k) {
     SlotDev<T> &S = tab[ids[GL_NEWTON * B + k]];
-    T *t = S.sig;
+    double *t = S.sig;
     S.sig = S.sig_next;
     S.sig_next = t;
   }
@@ -244,10 +244,10 @@ __global__ void group_decide_kernel(SlotDev<T> *tab, GroupCtl *ctl, int *ids, in
           c.state = GS_FAILED;
         } else if (conv) {
           // commit (update_state_variables; old_* <- current) by role swaps
-          T *t6;
-          t6 = S.sig_old; S.sig_old = S.sig; S.sig = t6;
-          t6 = S.eps_old; S.eps_old = S.eps; S.eps = t6;
-          t6 = S.kvox_old; S.kvox_old = S.kvox; S.kvox = t6;
+          double *f6;
+          f6 = S.sig_old; S.sig_old = S.sig; S.sig = f6;
+          f6 = S.eps_old; S.eps_old = S.eps; S.eps = f6;
+          T *t6 = S.kvox_old; S.kvox_old = S.kvox; S.kvox = t6;
           double *td;
           td = S.gam_old; S.gam_old = S.gam_trial; S.gam_trial = td;
           td = S.ep_old; S.ep_old = S.ep_trial; S.ep_trial = td;
@@ -688,7 +688,7 @@ struct Group {
       SlotDev<float> m;
       CK(cudaMemcpyAsync(&m, (char *)dtab + s * desc_bytes(), sizeof(m), cudaMemcpyDeviceToHost, stream));
       CK(cudaStreamSynchronize(stream));
-      to_point_major_kernel<float><<<eb, SSFFT_THREADS, 0, stream>>>(V, 6, m.sig_old, stage);
+      to_point_major_kernel<double><<<eb, SSFFT_THREADS, 0, stream>>>(V, 6, m.sig_old, stage);
     }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(dst, stage, (size_t)V * 6 * sizeof(double), cudaMemcpyDeviceToHost, stream));

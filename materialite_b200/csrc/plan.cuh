@@ -473,7 +473,7 @@ struct SlotBufs {
   bool fp64;
   size_t rs;                   // sizeof(real)
   long long V;
-  void *field[14];             // 6-plane fields: eps, eps_old, dfl, sig x3, b, kr[7]
+  void *field[14];             // 6-plane fields: eps, eps_old, dfl, sig x3 (double), b, kr[7]
   void *spec;
   double *partials;
   unsigned int *tickets;
@@ -506,14 +506,19 @@ static size_t field_bytes(const SlotBufs &b, int planes) {
   return (size_t)planes * (size_t)b.V * b.rs;
 }
 
+// Bytes of field[i]: the strain and stress fields (0..5) are double in both precisions.
+static size_t field_bytes_of(const SlotBufs &b, int i) {
+  return i < 6 ? (size_t)6 * (size_t)b.V * sizeof(double) : field_bytes(b, 6);
+}
+
 static int slot_alloc(SlotBufs &b, const GridPlan &p, cudaStream_t stream) {
   memset((void *)&b, 0, sizeof(b));
   b.fp64 = p.fp64;
   b.rs = p.fp64 ? 8 : 4;
   b.V = p.V;
   for (int i = 0; i < 14; ++i) {
-    ALLOC(b.field[i], field_bytes(b, 6));
-    CK(cudaMemsetAsync(b.field[i], 0, field_bytes(b, 6), stream));
+    ALLOC(b.field[i], field_bytes_of(b, i));
+    CK(cudaMemsetAsync(b.field[i], 0, field_bytes_of(b, i), stream));
   }
   ALLOC(b.spec, (size_t)6 * p.S * 16);  // sized for double-precision transforms
   ALLOC(b.partials, p.partial_doubles * sizeof(double));
@@ -547,12 +552,13 @@ template <typename T> static void mirror_init(SlotBufs &b, const ssfft_config &c
   SlotDev<T> &m = mirror<T>(b);
   memset((void *)&m, 0, sizeof(m));
   T **f = reinterpret_cast<T **>(b.field);
-  m.eps = f[0];
-  m.eps_old = f[1];
-  m.dfl = f[2];
-  m.sig = f[3];
-  m.sig_next = f[4];
-  m.sig_old = f[5];
+  double **fd = reinterpret_cast<double **>(b.field);
+  m.eps = fd[0];
+  m.eps_old = fd[1];
+  m.dfl = fd[2];
+  m.sig = fd[3];
+  m.sig_next = fd[4];
+  m.sig_old = fd[5];
   m.b = f[6];
   for (int i = 0; i < 7; ++i) m.kr[i] = f[7 + i];
   m.spec = b.spec;
@@ -780,7 +786,7 @@ static int slot_reset(SlotBufs &b, const ssfft_config &cfg, cudaStream_t stream)
     mirror_init<double>(b, cfg);
   else
     mirror_init<float>(b, cfg);
-  for (int i = 0; i < 7; ++i) CK(cudaMemsetAsync(b.field[i], 0, field_bytes(b, 6), stream));
+  for (int i = 0; i < 7; ++i) CK(cudaMemsetAsync(b.field[i], 0, field_bytes_of(b, i), stream));
   const long long V = b.V;
   const int eb = std::max(1, std::min(div_up(V, SSFFT_THREADS), 148 * 16));
   const int32_t *ph = b.have_phase_buf ? b.phase : nullptr;

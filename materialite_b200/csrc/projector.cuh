@@ -416,10 +416,10 @@ __device__ __forceinline__ void epilogue_point(const SlotDev<TF> &S, const ExtIO
       S.b[i] = (TF)r[q];
       acc0 = fmax(acc0, fabs((double)r[q]));
     } else if constexpr (EPI == EPI_REPROJECT) {
-      const TF x = (TF)r[q];
-      kr.X[i] = x;
-      S.eps[i] += x;
-      S.dfl[i] += x;
+      // the strain fields are double: they take the re-projected correction unrounded
+      kr.X[i] = (TF)r[q];
+      S.eps[i] += (double)r[q];
+      S.dfl[i] += (double)r[q];
     } else {  // EPI_PTAU
       kr.Y[i] = (TF)r[q];
     }

@@ -28,9 +28,11 @@ struct StepVec {
 enum { TK_INIT = 0, TK_ZINV, TK_UPD, TK_CONST, TK_NORMS, TK_TSUM, TK_COUNT };
 
 template <typename T> struct SlotDev {
-  // strain and stress fields, 6 component planes of V points each
-  T *eps, *eps_old, *dfl;       // strain, committed strain, accumulated fluctuation
-  T *sig, *sig_next, *sig_old;  // latest stress, constitutive output, committed stress
+  // strain and stress fields, 6 component planes of V points each, double in both
+  // precisions: the equilibrium residual is computed from them, and float storage would put
+  // its noise floor at the 1e-6 tolerance once stresses grow (Newton then stalls)
+  double *eps, *eps_old, *dfl;       // strain, committed strain, accumulated fluctuation
+  double *sig, *sig_next, *sig_old;  // latest stress, constitutive output, committed stress
   T *b;                         // equilibrium residual
   T *kr[7];                     // Krylov vectors; roles by iteration (kroles)
   void *spec;                   // half spectrum, sized for double-precision transforms

@@ -430,7 +430,8 @@ extern "C" int ssfft_estimate_bytes(const ssfft_config *cfg, int any_evp, int n_
   const size_t V = (size_t)cfg->n[0] * cfg->n[1] * cfg->n[2];
   const size_t rs = cfg->precision == SSFFT_FP64 ? 8 : 4;
   const size_t S = (size_t)cfg->n[0] * cfg->n[1] * (cfg->n[2] / 2 + 1);
-  size_t b = 14 * 6 * V * rs + 6 * S * 16 + 3 * V * 4;
+  // strain and stress fields double in both precisions, the rest in the solve precision
+  size_t b = 6 * 6 * V * 8 + 8 * 6 * V * rs + 6 * S * 16 + 3 * V * 4;
   if (any_evp) b += 2 * 21 * V * rs + (5 * (size_t)n_slip + 12 + 2) * V * 8;
   b += (size_t)21 * ((V + VEC_CHUNK - 1) / VEC_CHUNK + 1) * 8 + 3 * 3 * (size_t)cfg->n[0] * 8;
   b += (size_t)1 << 20;  // tables, scalars, orientation table
@@ -658,10 +659,9 @@ extern "C" int ssfft_scale_fluctuation(ssfft_handle *h, double factor) {
   const long long n = 6 * h->plan.V;
   const int eb = std::max(1, std::min(div_up(n, SSFFT_THREADS), 148 * 16));
   if (factor != 1.0) {
-    if (h->plan.fp64)
-      scale_kernel<double><<<eb, SSFFT_THREADS, 0, h->stream>>>(n, h->sb.md.dfl, factor);
-    else
-      scale_kernel<float><<<eb, SSFFT_THREADS, 0, h->stream>>>(n, h->sb.mf.dfl, factor);
+    // the fluctuation field is double in both precisions
+    double *dfl = h->plan.fp64 ? h->sb.md.dfl : h->sb.mf.dfl;
+    scale_kernel<double><<<eb, SSFFT_THREADS, 0, h->stream>>>(n, dfl, factor);
     CK(cudaGetLastError());
   }
   return 0;  // ordered on the handle's stream; no host synchronisation needed
@@ -757,8 +757,14 @@ static int read_field(const SlotBufs &b, const SlotDev<T> &m, bool committed, in
   *width = 6;
   *is_double = false;
   switch (field) {
-    case SSFFT_FIELD_STRESS: *src = committed ? m.sig_old : m.sig; return 0;
-    case SSFFT_FIELD_STRAIN: *src = committed ? m.eps_old : m.eps; return 0;
+    case SSFFT_FIELD_STRESS:  // stress and strain are double in both precisions
+      *is_double = true;
+      *src = committed ? m.sig_old : m.sig;
+      return 0;
+    case SSFFT_FIELD_STRAIN:
+      *is_double = true;
+      *src = committed ? m.eps_old : m.eps;
+      return 0;
     case SSFFT_FIELD_RESIDUAL: *src = m.b; return 0;
     case SSFFT_FIELD_SLIP_RESISTANCES:
     case SSFFT_FIELD_SLIP_SHEAR_STRAINS:
