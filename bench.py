@@ -64,7 +64,7 @@ WORKLOADS = {
     # stream's 32^3 elastic requests among the first `cpu_count` (the CPU-feasible class,
     # solved in full by the CPU baselines).
     "serve": dict(count=512, rate=50.0, slots=16, seed=1000, sweep_rates=(1, 2, 5, 10, 20),
-                  sweep_seconds=20.0, plain_count=48, e2e_count=128, cpu_count=512),
+                  sweep_seconds=20.0, plain_count=128, e2e_count=128, cpu_count=512),
 }
 
 def plane_path(n):
@@ -453,7 +453,8 @@ def serve_mode(args, w):
         return comps, span
 
     import torch
-    srv = RVEServer(device=local, max_slots=w["slots"], precision="mixed")
+    srv = RVEServer(device=local, max_slots=w["slots"], precision="mixed",
+                    krylov_floor=args.krylov_floor)
     warm = list(classes.values())
     for _ in range(args.warmup):
         one_pass(srv, warm, False, saturate=True)
@@ -493,10 +494,11 @@ def serve_mode(args, w):
     # plain single-request FP64 GPU solve of a prefix, against the served mixed solve of the
     # same requests (all submitted at once)
     sub = reqs[:min(len(reqs), w["plain_count"])]
-    _, span_sub = one_pass(srv, sub, True, saturate=True)
+    comps_sub, span_sub = one_pass(srv, sub, True, saturate=True)
     stress_mixed = [r.stress.copy() for r in sub]
+    krylov_floor = srv.krylov_floor
     srv.close()
-    secs_plain, _ = solve_plain(sub, "fp64", device=local)
+    secs_plain, pouts = solve_plain(sub, "fp64", device=local)
     stress_fp64 = [r.stress.copy() for r in sub]
     errs = [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(stress_mixed, stress_fp64)]
     plain_value = len(sub) / sum(secs_plain)
@@ -506,7 +508,8 @@ def serve_mode(args, w):
     cpu_reqs = [r for r in reqs if r.tag in cpu_tags]
     cpu_gpu = None
     if cpu_reqs:
-        srv2 = RVEServer(device=local, max_slots=w["slots"], precision="mixed")
+        srv2 = RVEServer(device=local, max_slots=w["slots"], precision="mixed",
+                         krylov_floor=args.krylov_floor)
         _, span_c = one_pass(srv2, cpu_reqs, False, saturate=True)
         srv2.close()
         secs_c, _ = solve_plain(cpu_reqs, "fp64", device=local, keep_stress=False)
@@ -525,8 +528,10 @@ def serve_mode(args, w):
                        "requests_per_step": per_step,
                        "parallelism": f"replicas x{world} (stream partitioned by cost)",
                        "slots_per_class": w["slots"], "voxels": voxels,
-                       "precision": "float fields and FFTs; double residuals, norms, Krylov "
-                                    "scalars and crystal-plasticity Newton",
+                       "precision": "float Krylov vectors, tangents and matvec FFTs; double "
+                                    "strain/stress fields, residuals, norms, Krylov scalars "
+                                    "and crystal-plasticity Newton",
+                       "krylov_floor": krylov_floor,
                        "l2": "inputs larger than L2: the stream's fields stream through HBM"},
             "served": {"solves_per_s": value, **lat, "makespan_s": t_max,
                        "per_class_latency": per_class},
@@ -534,7 +539,13 @@ def serve_mode(args, w):
             "plain_fp64_single_request": {"workload": f"first {len(sub)} requests of the "
                                                       "stream, one at a time",
                                           "solves_per_s": plain_value,
-                                          "served_solves_per_s_same_requests": served_sub},
+                                          "served_solves_per_s_same_requests": served_sub,
+                                          "newton": int(sum(o.newton_iterations for o in pouts)),
+                                          "krylov": int(sum(o.krylov_iterations for o in pouts)),
+                                          "served_newton": int(sum(c.result.newton_iterations
+                                                                   for c in comps_sub)),
+                                          "served_krylov": int(sum(c.result.krylov_iterations
+                                                                   for c in comps_sub))},
             # the same requests both ways; the served side is all of them at once, so its
             # makespan ends with the longest request (a tail the one-at-a-time sum has not)
             "served_over_plain": served_sub / plain_value,
@@ -573,7 +584,8 @@ def sweep_mode(args, w):
     from materialite_b200.serving import RVEServer, latency_stats, request_stream, run_stream
     count = args.count or 64
     rates = [float(x) for x in args.rates.split(",")]
-    srv = RVEServer(device=0, max_slots=w["slots"], precision="mixed")
+    srv = RVEServer(device=0, max_slots=w["slots"], precision="mixed",
+                    krylov_floor=args.krylov_floor)
     run_stream(srv, request_stream(min(count, 8), 0.0, seed=w["seed"]), timeout=1800)
     out = {"workload": f"serve sweep: {count} requests of the serving stream, "
                        f"{w['slots']} slots per class, mixed precision", "rates": []}
@@ -607,7 +619,8 @@ def classes_mode(args, w):
         rs = by[kind]
         secs, pouts = solve_plain(rs, precision="fp64", device=0, keep_stress=True)
         ref = [r.stress.copy() for r in rs]
-        srv = RVEServer(device=0, max_slots=w["slots"], precision="mixed")
+        srv = RVEServer(device=0, max_slots=w["slots"], precision="mixed",
+                        krylov_floor=args.krylov_floor)
         for r in rs:
             r.keep_stress = True
             r.arrival = 0.0
@@ -641,7 +654,8 @@ def group_mode(args, w):
             tags.append(t)
         t += 1
     reqs = request_stream(len(tags), w["rate"], seed=w["seed"], workers=host_workers(), tags=tags)
-    srv = RVEServer(device=0, max_slots=w["slots"], precision=args.precision)
+    srv = RVEServer(device=0, max_slots=w["slots"], precision=args.precision,
+                    krylov_floor=args.krylov_floor)
     for r in reqs:
         r.arrival = 0.0
     comps, span = run_stream(srv, reqs, timeout=3600)
@@ -793,6 +807,9 @@ def main():
     ap.add_argument("--tag", type=int, default=0, help="request mode: index in the stream")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--kind", default="evp64", help="group mode: request class (e.g. evp64)")
+    ap.add_argument("--krylov-floor", type=float, default=None,
+                    help="served requests' MINRES floor (fraction of the tolerance); "
+                         "default: the server's (0.1 mixed, 0 FP64)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.mode == "kernels":

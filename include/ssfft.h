@@ -78,6 +78,13 @@ typedef struct {
   double strain_correction_tolerance; /* default 1e-2 */
   double linear_solver_tolerance; /* default 1e-5 */
   double stress_mask[6];          /* 0/1 per Mandel component */
+  /* Absolute floor of the MINRES stopping test, as a fraction of global_tolerance: a
+   * solve also stops once its residual |b - A x|_2 is at most
+   * krylov_floor * global_tolerance * (mean von Mises stress).  For a linear material the
+   * next equilibrium residual is that MINRES residual, and max|r| <= |r|_2, so the floor
+   * keeps the next equilibrium error at or below krylov_floor * global_tolerance.  0 (the
+   * reference's test alone, small_strain_fft.py:289-293) unless set. */
+  double krylov_floor;
 } ssfft_config;
 
 /* Per load step inputs: the LoadSchedule closures evaluated at (t, dt)

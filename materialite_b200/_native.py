@@ -58,6 +58,7 @@ class SsfftConfig(ctypes.Structure):
         ("strain_correction_tolerance", ctypes.c_double),
         ("linear_solver_tolerance", ctypes.c_double),
         ("stress_mask", ctypes.c_double * 6),
+        ("krylov_floor", ctypes.c_double),
     ]
 
 

@@ -217,6 +217,30 @@ __device__ __forceinline__ double ordered_max(const double *p, int count, int st
   return block_max(v, scratch);
 }
 
+// Product rounded on its own on the device as well (no fused multiply-add), so that the
+// Newton decisions taken on the device (serving groups) and on the host (handles) agree
+// to the last bit.
+__host__ __device__ inline double mul_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+
+// Mean von Mises stress from summed stress components (small_strain_fft.py:141-143).
+__host__ __device__ inline double mean_von_mises(const double *sums, long long V) {
+  double m[6];
+  for (int c = 0; c < 6; ++c) m[c] = sums[c] / (double)V;
+  const double tr3 = (m[0] + m[1] + m[2]) / 3.0;
+  double s = 0.0;
+  for (int c = 0; c < 6; ++c) {
+    const double d = (c < 3) ? m[c] - tr3 : m[c];
+    s += mul_rn(d, d);
+  }
+  return sqrt(s) * sqrt(1.5);
+}
+
 // Symmetric 6x6 packed as 21 entries, upper triangle row by row:
 // (0,0)(0,1)..(0,5)(1,1)..(1,5)(2,2)..(5,5)
 __host__ __device__ __forceinline__ int sym_idx(int i, int j) {

@@ -607,11 +607,13 @@ struct Group {
     if (plan.fp64) {
       b.md.rtol = cfg.linear_solver_tolerance;
       b.md.maxiter = maxiter;
+      b.md.atol_scale = krylov_atol_scale(cfg);
       CK(cudaMemcpyAsync((char *)dtab + s * desc_bytes(), &b.md, sizeof(b.md),
                          cudaMemcpyHostToDevice, stream));
     } else {
       b.mf.rtol = std::max(cfg.linear_solver_tolerance, MIXED_RTOL_FLOOR);
       b.mf.maxiter = maxiter;
+      b.mf.atol_scale = krylov_atol_scale(cfg);
       CK(cudaMemcpyAsync((char *)dtab + s * desc_bytes(), &b.mf, sizeof(b.mf),
                          cudaMemcpyHostToDevice, stream));
     }

@@ -307,6 +307,8 @@ static int validate_config(const ssfft_config *cfg) {
   for (int c = 0; c < 6; ++c)
     if (cfg->stress_mask[c] != 0.0 && cfg->stress_mask[c] != 1.0)
       return ssfft_internal_fail(SSFFT_E_INVALID, "stress mask can only have zeros and ones");
+  if (!(cfg->krylov_floor >= 0.0 && cfg->krylov_floor < 1.0))
+    return ssfft_internal_fail(SSFFT_E_INVALID, "krylov_floor must be in [0, 1)");
   AxisPlan p;
   for (int d = 0; d < 3; ++d)
     if (!make_axis_plan(cfg->n[d], p))
@@ -1041,16 +1043,6 @@ static int launch_commit_slip(const LaunchCtx &c, const SlotDev<T> *tab, int nsl
   return 0;
 }
 
-// Product rounded on its own on the device as well (no fused multiply-add), so that the
-// Newton decisions taken on the device (serving groups) and on the host (handles) agree
-// to the last bit.
-__host__ __device__ inline double mul_rn(double a, double b) {
-#ifdef __CUDA_ARCH__
-  return __dmul_rn(a, b);
-#else
-  return a * b;
-#endif
-}
 
 // 6x6 inverse by Gauss-Jordan with partial pivoting (host and device, double).
 __host__ __device__ inline bool inv6(const double *A, double *Ainv) {
@@ -1082,15 +1074,3 @@ __host__ __device__ inline bool inv6(const double *A, double *Ainv) {
   return true;
 }
 
-// Mean von Mises stress from summed stress components (small_strain_fft.py:141-143).
-__host__ __device__ inline double mean_von_mises(const double *sums, long long V) {
-  double m[6];
-  for (int c = 0; c < 6; ++c) m[c] = sums[c] / (double)V;
-  const double tr3 = (m[0] + m[1] + m[2]) / 3.0;
-  double s = 0.0;
-  for (int c = 0; c < 6; ++c) {
-    const double d = (c < 3) ? m[c] - tr3 : m[c];
-    s += mul_rn(d, d);
-  }
-  return sqrt(s) * sqrt(1.5);
-}

@@ -126,7 +126,7 @@ struct MinresState {
   double beta1, beta, oldb, alfa, dbar, epsln, phibar, tnorm2, gmax, gmin, cs, sn;
   double delta, oldeps, gamma, phi, denom, root, anorm, ynorm, rnorm, test1, test2;
   double s, s_prev, c_r1, coef;
-  double rtol, eps;
+  double rtol, eps, atol;
   long long itn, maxiter;
   int istop, done;
 };
@@ -183,6 +183,7 @@ static __device__ __noinline__ void minres_after_update(MinresState *st, double 
     if (epsx >= s.beta1) s.istop = 3;
     if (s.test2 <= s.rtol) s.istop = 2;
     if (s.test1 <= s.rtol) s.istop = 1;
+    if (s.rnorm <= s.atol) s.istop = 1;  // the absolute floor (0 when off)
   }
   if (!isfinite(s.ynorm) || !isfinite(s.beta)) s.istop = 9;  // NaN guard
   if (s.beta == 0.0 && s.istop == 0) s.istop = 1;           // exact breakdown

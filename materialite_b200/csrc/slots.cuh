@@ -69,6 +69,8 @@ template <typename T> struct SlotDev {
   double dt;
   double rtol;                  // MINRES relative tolerance and iteration limit
   long long maxiter;
+  double atol_scale;            // MINRES also stops once |r| <= atol_scale x mean von Mises
+                                // stress (0: off)
 };
 
 // The slots a launch works on: ids[0 .. *count).  Both live in device memory, so a kernel

@@ -115,6 +115,11 @@ static void drop_graph(ssfft_handle *h) {
 #define KRYLOV_CHUNK 6
 #define MIXED_RTOL_FLOOR 1.0e-6
 
+// The MINRES absolute floor per unit of mean von Mises stress (ssfft_config::krylov_floor).
+static inline double krylov_atol_scale(const ssfft_config &cfg) {
+  return cfg.krylov_floor > 0.0 ? cfg.krylov_floor * cfg.global_tolerance : 0.0;
+}
+
 template <typename T> static int run_minres(ssfft_handle *h, long long *iters) {
   NvtxScope range("ssfft_minres");
   const LaunchCtx c = ctx(h);
@@ -320,6 +325,7 @@ template <typename T> static int step_impl(ssfft_handle *h, const ssfft_step_in 
   // float Krylov vectors cannot resolve relative residuals much below 1e-6
   m.rtol = h->plan.fp64 ? h->cfg.linear_solver_tolerance
                         : std::max(h->cfg.linear_solver_tolerance, MIXED_RTOL_FLOOR);
+  m.atol_scale = krylov_atol_scale(h->cfg);
   CKR(upload(h));
   CKR(launch_strain_guess<T>(c, dtab<T>(h)));
 
@@ -920,6 +926,7 @@ template <typename T> static int profile_impl(ssfft_handle *h, int reps, double 
   m.sig = m.sig_old;
   for (int k = 0; k < 6; ++k) m.sbar[k] = 0.0;
   m.rtol = 0.0;
+  m.atol_scale = 0.0;
   m.maxiter = (long long)1 << 60;
   CKR(upload(h));
   CKR(launch_residual<T>(c, dtab<T>(h)));

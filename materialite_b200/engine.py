@@ -64,7 +64,10 @@ class SolverHandle:
 
     def __init__(self, dims, stress_mask, precision="mixed", global_tolerance=1.0e-3,
                  strain_correction_tolerance=1.0e-2, linear_solver_tolerance=1.0e-5,
-                 max_newton_iterations=100, max_krylov_iterations=0, device=0):
+                 max_newton_iterations=100, max_krylov_iterations=0, device=0,
+                 krylov_floor=0.0):
+        """``krylov_floor`` > 0 adds an absolute floor to the MINRES stopping test
+        (ssfft_config.krylov_floor); 0 keeps the reference's test alone."""
         self.lib = nat.load_library()
         cfg = nat.SsfftConfig()
         for d in range(3):
@@ -76,6 +79,7 @@ class SolverHandle:
         cfg.global_tolerance = float(global_tolerance)
         cfg.strain_correction_tolerance = float(strain_correction_tolerance)
         cfg.linear_solver_tolerance = float(linear_solver_tolerance)
+        cfg.krylov_floor = float(krylov_floor)
         for c in range(6):
             cfg.stress_mask[c] = float(stress_mask[c])
         self.cfg = cfg
@@ -148,7 +152,8 @@ class SolverHandle:
         nat.check(self.lib.ssfft_reset(self.h))
 
     def set_options(self, stress_mask=None, global_tolerance=None,
-                    strain_correction_tolerance=None, linear_solver_tolerance=None):
+                    strain_correction_tolerance=None, linear_solver_tolerance=None,
+                    krylov_floor=None):
         """Change the stress mask and tolerances of the handle (same grid and precision)."""
         cfg = self.cfg
         if stress_mask is not None:
@@ -160,6 +165,8 @@ class SolverHandle:
             cfg.strain_correction_tolerance = float(strain_correction_tolerance)
         if linear_solver_tolerance is not None:
             cfg.linear_solver_tolerance = float(linear_solver_tolerance)
+        if krylov_floor is not None:
+            cfg.krylov_floor = float(krylov_floor)
         nat.check(self.lib.ssfft_set_options(self.h, ctypes.byref(cfg)))
 
     def solve_constant_rates(self, strain_rate, stress_rate, end_time, initial_time_increment,

@@ -18,6 +18,13 @@ from . import _native as nat
 from .engine import hardening_props_vector
 from .microstructure import periodic_voronoi, quaternion_random_rotations
 
+# MINRES absolute floor of served mixed-precision requests, as a fraction of the global
+# tolerance: a linear solve stops once its residual could move the next equilibrium error
+# by at most a tenth of the tolerance.  An elastic request's later increments then start
+# at equilibrium to round-off and need no Krylov iterations, where the reference's relative
+# test spends 30-45 iterations resolving that round-off.
+SERVED_KRYLOV_FLOOR = 0.1
+
 
 class SsfftPhase(ctypes.Structure):
     _fields_ = [
@@ -121,13 +128,20 @@ def _phase_struct(p):
 
 
 class RVEServer:
-    def __init__(self, device=0, max_slots=16, hbm_budget_bytes=0, precision="mixed"):
+    def __init__(self, device=0, max_slots=16, hbm_budget_bytes=0, precision="mixed",
+                 krylov_floor=None):
+        """``krylov_floor``: the MINRES absolute floor of every request
+        (ssfft_config.krylov_floor); None gives SERVED_KRYLOV_FLOOR in mixed precision and 0
+        (the reference's stopping test alone) in FP64."""
         self.lib = _bind(nat.load_library())
         h = ctypes.c_void_p()
         nat.check(self.lib.ssfft_server_create(int(device), int(max_slots),
                                                 int(hbm_budget_bytes), ctypes.byref(h)))
         self.h = h
         self.precision = precision
+        if krylov_floor is None:
+            krylov_floor = SERVED_KRYLOV_FLOOR if precision != "fp64" else 0.0
+        self.krylov_floor = float(krylov_floor)
         self._keep = {}
 
     def clock(self):
@@ -143,6 +157,7 @@ class RVEServer:
         cfg.global_tolerance = r.global_tolerance
         cfg.strain_correction_tolerance = 1e-2
         cfg.linear_solver_tolerance = r.linear_solver_tolerance
+        cfg.krylov_floor = self.krylov_floor
         for c in range(6):
             cfg.stress_mask[c] = float(r.stress_mask[c])
         req.n_phases = len(r.phases)

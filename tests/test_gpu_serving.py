@@ -6,8 +6,8 @@ import numpy as np
 import pytest
 
 from materialite_b200.engine import SolverHandle, solve, unique_rotations
-from materialite_b200.serving import (RVEServer, elastic_phase, evp_phase, make_request,
-                                      run_stream)
+from materialite_b200.serving import (SERVED_KRYLOV_FLOOR, RVEServer, elastic_phase,
+                                      evp_phase, make_request, run_stream, solve_plain)
 
 pytestmark = pytest.mark.gpu
 
@@ -51,7 +51,8 @@ def test_native_time_loop_matches_python_loop():
     server.close()
     assert comps[0].status == 0
     h = SolverHandle(r.dims, r.stress_mask, "mixed", global_tolerance=r.global_tolerance,
-                     linear_solver_tolerance=r.linear_solver_tolerance)
+                     linear_solver_tolerance=r.linear_solver_tolerance,
+                     krylov_floor=SERVED_KRYLOV_FLOOR)
     h.set_phases(r.phases)
     table, idx = unique_rotations(r.rotations[r.grain])
     h.set_microstructure(table, idx)
@@ -132,7 +133,8 @@ def test_group_time_loop_matches_python_loop_crystal_plasticity():
     server.close()
     assert comps[0].status == 0
     h = SolverHandle(r.dims, r.stress_mask, "mixed", global_tolerance=r.global_tolerance,
-                     linear_solver_tolerance=r.linear_solver_tolerance)
+                     linear_solver_tolerance=r.linear_solver_tolerance,
+                     krylov_floor=SERVED_KRYLOV_FLOOR)
     h.set_phases(r.phases)
     table, idx = unique_rotations(r.rotations[r.grain])
     h.set_microstructure(table, idx)
@@ -167,3 +169,28 @@ def test_late_request_joins_a_running_group():
     assert b.submit_time > a.start_time          # the long request was running
     assert b.end_time < a.end_time               # and the short one did not wait for it
     assert np.array_equal(short_r.stress, alone.stress)
+
+
+def test_krylov_floor_keeps_the_fp64_result():
+    """The served mixed form's MINRES floor (a linear solve stops once its residual could
+    move the next equilibrium error by a tenth of the tolerance): an elastic request's later
+    increments start at equilibrium to round-off and take no Krylov iterations, and a
+    crystal-plasticity request stops its last linear solves early; both stay within 1e-6
+    of the plain FP64 solve, which keeps the reference's stopping test alone."""
+    reqs = small_requests()[:2]  # one elastic, one crystal-plasticity request
+    plain = small_requests()[:2]
+    _, pouts = solve_plain(plain, precision="fp64")
+    server = RVEServer(max_slots=2)
+    comps, _ = run_stream(server, reqs)
+    server.close()
+    comps = sorted(comps, key=lambda c: c.tag)
+    for r, p, c, po in zip(reqs, plain, comps, pouts):
+        assert c.status == 0
+        assert c.result.steps == po.steps and c.result.cutbacks == po.cutbacks
+        err = np.linalg.norm(r.stress - p.stress) / np.linalg.norm(p.stress)
+        assert err <= 1e-6, (r.tag, err)
+        assert c.result.krylov_iterations < po.krylov_iterations
+    elastic, plain_elastic = comps[0].result, pouts[0]
+    # only the first increment has a residual above round-off
+    assert elastic.krylov_iterations * 2 < plain_elastic.krylov_iterations
+    assert elastic.newton_iterations == plain_elastic.newton_iterations

@@ -67,6 +67,15 @@ def test_config_validation(n, mask, code):
     assert nat.load_library().ssfft_last_error()
 
 
+@pytest.mark.parametrize("floor", [-0.1, 1.0, float("nan")])
+def test_krylov_floor_validation(floor):
+    cfg = config()
+    cfg.krylov_floor = floor
+    rc, _ = estimate(cfg)
+    assert rc == -1
+    assert b"krylov_floor" in nat.load_library().ssfft_last_error()
+
+
 def test_invalid_precision_rejected():
     rc, _ = estimate(config(precision=7))
     assert rc == -1
