@@ -164,6 +164,7 @@ struct GridPlan {
   long long V, S;             // points; stored half-spectrum points
   AxisPlan px, py, pz;
   int lz, ky, kx;
+  int kx_f;                   // kz columns per x-pass tile of the float transforms
   bool use_plane;             // plane-fused passes allowed (SSFFT_NO_PLANE=1 forbids)
   void *tw[2][3], *tn[2][3];  // [0]: float, [1]: double tables per axis
   Grid<float> gf;
@@ -227,7 +228,7 @@ template <typename T> static void fill_grid(GridPlan &p) {
   g.scale = (T)(1.0 / (double)p.V);
   g.lz = p.lz;
   g.ky = p.ky;
-  g.kx = p.kx;
+  g.kx = sizeof(T) == 4 ? p.kx_f : p.kx;
   grid_divisors(g);
 }
 
@@ -276,14 +277,41 @@ template <typename T> static ClusterGeo cluster_geo(const GridPlan &p, int C) {
 }
 
 // Threads of a cluster block: 512 when two blocks fit an SM's shared memory, else 1024
-// (SSFFT_CLUSTER_THREADS=512 or 1024 overrides where the memory allows).
+// (SSFFT_CLUSTER_THREADS=256, 512 or 1024 overrides).
 template <typename T> static int cluster_threads(const GridPlan &p, int C) {
   const int hs = (p.nz % 2 == 0) ? p.nz / 2 : p.hz;
   const bool two = smem_cplane_bytes<T>(p.ny, p.nz, hs, C) <= 113 * 1024;
   const int want = env_int("SSFFT_CLUSTER_THREADS");
-  if (want == 1024) return 1024;
-  if (want == 512) return 512;
+  if (want == 1024 || want == 512 || want == 256) return want;
   return two ? 512 : 1024;
+}
+
+// Threads of an x-pass block: 256, or 192 / 384 on float grids when SSFFT_XPASS_THREADS
+// asks for them.
+template <typename T> static int xpass_threads() {
+  if (sizeof(T) != 4) return XPASS_THREADS;
+  const int want = env_int("SSFFT_XPASS_THREADS");
+  return (want == 192 || want == 384) ? want : XPASS_THREADS;
+}
+
+template <typename T, typename TF, bool KRY>
+static void launch_xpass(const Grid<T> &g, size_t sx, long long items, int dev,
+                         cudaStream_t stream, const SlotDev<TF> *tab, SlotList list) {
+  const int pt = xpass_threads<T>();
+  if constexpr (sizeof(T) == 4) {
+    if (pt == 384) {
+      auto k = xpass_kernel<T, TF, KRY, 384>;
+      k<<<persistent_grid(k, 384, sx, items, dev), 384, sx, stream>>>(g, tab, list);
+      return;
+    }
+    if (pt == 192) {
+      auto k = xpass_kernel<T, TF, KRY, 192>;
+      k<<<persistent_grid(k, 192, sx, items, dev), 192, sx, stream>>>(g, tab, list);
+      return;
+    }
+  }
+  auto k = xpass_kernel<T, TF, KRY>;
+  k<<<persistent_grid(k, XPASS_THREADS, sx, items, dev), XPASS_THREADS, sx, stream>>>(g, tab, list);
 }
 
 // The projection runs as three passes (z and y fused, in one block or one cluster).
@@ -327,6 +355,13 @@ static int plan_tiles(GridPlan &p) {
   // to 64 points along x, where 8 would leave about two blocks per SM
   p.kx = std::min(p.hz, p.nx <= 64 ? 4 : 8);
   while (p.kx > 1 && smem_x_bytes<double>(p.kx, p.nx) > 100 * 1024) p.kx /= 2;
+  // float x tiles: the double tile unless SSFFT_XPASS_KX asks for another power of two
+  // that fits
+  p.kx_f = p.kx;
+  const int want_kx = env_int("SSFFT_XPASS_KX");
+  if (want_kx >= 1 && want_kx <= 32 && (want_kx & (want_kx - 1)) == 0 &&
+      smem_x_bytes<float>(std::min(want_kx, p.hz), p.nx) <= SMEM_LIMIT)
+    p.kx_f = std::min(want_kx, p.hz);
   if (smem_z_bytes<double>(p.lz, p.nz) > SMEM_LIMIT || smem_y_bytes<double>(p.ky, p.ny) > SMEM_LIMIT ||
       smem_x_bytes<double>(p.kx, p.nx) > SMEM_LIMIT)
     return ssfft_internal_fail(SSFFT_E_UNSUPPORTED, "grid too large for the shared-memory FFT passes");
@@ -451,11 +486,18 @@ template <typename T, typename TF> static int set_kernel_attrs(size_t smax) {
   CKR((smem_attr(ypass_kernel<T, TF, true, true>, m)));
   CKR((smem_attr(xpass_kernel<T, TF, false>, m)));
   CKR((smem_attr(xpass_kernel<T, TF, true>, m)));
+  if constexpr (sizeof(T) == 4) {
+    CKR((smem_attr(xpass_kernel<T, TF, false, 192>, m)));
+    CKR((smem_attr(xpass_kernel<T, TF, true, 192>, m)));
+    CKR((smem_attr(xpass_kernel<T, TF, false, 384>, m)));
+    CKR((smem_attr(xpass_kernel<T, TF, true, 384>, m)));
+  }
   CKR(smem_attr(zinv_kernel<T, TF, EPI_STORE>, m));
   CKR(smem_attr(zinv_kernel<T, TF, EPI_RESIDUAL>, m));
   CKR(smem_attr(zinv_kernel<T, TF, EPI_REPROJECT>, m));
   CKR((plane_attrs<T, TF, 512>(m)));
   CKR((plane_attrs<T, TF, 1024>(m)));
+  CKR((cluster_attrs<T, TF, 256>(m)));
   CKR((cluster_attrs<T, TF, 512>(m)));
   CKR((cluster_attrs<T, TF, 1024>(m)));
   if (sizeof(T) == sizeof(TF)) {
@@ -846,7 +888,7 @@ static int launch_projector(const LaunchCtx &c, const SlotDev<TF> *tab, ExtIO<TF
   auto rec = [&](int k) {
     if (ev) cudaEventRecord(ev[k], c.stream);
   };
-  const size_t sx = smem_x_bytes<T>(p.kx, p.nx);
+  const size_t sx = smem_x_bytes<T>(g.kx, p.nx);
   const int dev = p.dev;
   rec(0);
   if (const int C = cluster_size<T>(p)) {
@@ -856,17 +898,19 @@ static int launch_projector(const LaunchCtx &c, const SlotDev<TF> *tab, ExtIO<TF
     const int pt = cluster_threads<T>(p, C);
     if (pt == 1024)
       CKR(launch_clustered(zyfwd_cl_kernel<T, TF, PRO, 1024>, C, 1024, sp, it, dev, c.stream, g, q, tab, c.list, io));
+    else if (pt == 256)
+      CKR(launch_clustered(zyfwd_cl_kernel<T, TF, PRO, 256>, C, 256, sp, it, dev, c.stream, g, q, tab, c.list, io));
     else
       CKR(launch_clustered(zyfwd_cl_kernel<T, TF, PRO, 512>, C, 512, sp, it, dev, c.stream, g, q, tab, c.list, io));
     rec(1);
     rec(2);
-    auto kx = xpass_kernel<T, TF, KRY>;
-    kx<<<persistent_grid(kx, XPASS_THREADS, sx, (long long)c.cap * items_x(g), dev), XPASS_THREADS,
-         sx, c.stream>>>(g, tab, c.list);
+    launch_xpass<T, TF, KRY>(g, sx, (long long)c.cap * items_x(g), dev, c.stream, tab, c.list);
     rec(3);
     rec(4);
     if (pt == 1024)
       CKR(launch_clustered(yzinv_cl_kernel<T, TF, EPI, 1024>, C, 1024, sp, it, dev, c.stream, g, q, tab, c.list, io));
+    else if (pt == 256)
+      CKR(launch_clustered(yzinv_cl_kernel<T, TF, EPI, 256>, C, 256, sp, it, dev, c.stream, g, q, tab, c.list, io));
     else
       CKR(launch_clustered(yzinv_cl_kernel<T, TF, EPI, 512>, C, 512, sp, it, dev, c.stream, g, q, tab, c.list, io));
     rec(5);
@@ -883,9 +927,7 @@ static int launch_projector(const LaunchCtx &c, const SlotDev<TF> *tab, ExtIO<TF
     }
     rec(1);
     rec(2);
-    auto kx = xpass_kernel<T, TF, KRY>;
-    kx<<<persistent_grid(kx, XPASS_THREADS, sx, (long long)c.cap * items_x(g), dev), XPASS_THREADS,
-         sx, c.stream>>>(g, tab, c.list);
+    launch_xpass<T, TF, KRY>(g, sx, (long long)c.cap * items_x(g), dev, c.stream, tab, c.list);
     rec(3);
     rec(4);
     if (plane_threads<T>(p) == 1024) {
@@ -908,9 +950,7 @@ static int launch_projector(const LaunchCtx &c, const SlotDev<TF> *tab, ExtIO<TF
     auto ky = ypass_kernel<T, TF, false, KRY>;
     ky<<<persistent_grid(ky, SSFFT_THREADS, sy, ity, dev), SSFFT_THREADS, sy, c.stream>>>(g, tab, c.list);
     rec(2);
-    auto kx = xpass_kernel<T, TF, KRY>;
-    kx<<<persistent_grid(kx, XPASS_THREADS, sx, (long long)c.cap * items_x(g), dev), XPASS_THREADS,
-         sx, c.stream>>>(g, tab, c.list);
+    launch_xpass<T, TF, KRY>(g, sx, (long long)c.cap * items_x(g), dev, c.stream, tab, c.list);
     rec(3);
     auto kyi = ypass_kernel<T, TF, true, KRY>;
     kyi<<<persistent_grid(kyi, SSFFT_THREADS, sy, ity, dev), SSFFT_THREADS, sy, c.stream>>>(g, tab, c.list);

@@ -641,9 +641,10 @@ __device__ __forceinline__ void green_apply(const Grid<T> &g, const double *mask
 
 // x pass: an item is (slot, y, kz column tile); forward x-FFT of all six components,
 // Gamma-hat, inverse x-FFT, store.  KRY: skip slots whose solve is done.
+// PT threads a block (any multiple of 32 up to 1024: every loop strides by blockDim.x).
 #define XPASS_THREADS SSFFT_THREADS
-template <typename T, typename TF, bool KRY>
-__global__ void __launch_bounds__(XPASS_THREADS)
+template <typename T, typename TF, bool KRY, int PT = XPASS_THREADS>
+__global__ void __launch_bounds__(PT)
     xpass_kernel(Grid<T> g, const SlotDev<TF> *__restrict__ tab, SlotList list) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nx = g.nx, ny = g.ny, hs = g.hs;
@@ -819,9 +820,8 @@ template <typename T> inline size_t smem_plane_bytes(int ny, int nz) {
   return (2 * (size_t)padded_len(ny * (nz + 2)) + ny + nz) * sizeof(cplx<T>);
 }
 
-// Plane kernels run PT threads (512 or 1024; a plane holds too few blocks per SM to
-// hide memory latency with fewer warps), at most 64 registers each.
-#define PLANE_MIN_BLOCKS(PT) ((PT) >= 1024 ? 1 : 2)
+// Plane kernels run PT threads (256, 512 or 1024), at most 64 registers each.
+#define PLANE_MIN_BLOCKS(PT) (1024 / (PT))
 
 // Prologue of a plane item over the points vbase .. vbase + nel - 1 (whole z lines): tau
 // of the component pair p as one complex value per point, into padded z lines in buf.
@@ -1016,8 +1016,9 @@ template <typename T> inline size_t smem_cplane_bytes(int ny, int nz, int hs, in
   return (2 * (size_t)cplane_buf_elems(ny, nz, hs, C) + ny + nz) * sizeof(cplx<T>);
 }
 
-// Blocks of PT = 1024 threads (one per SM) or 512 (two per SM when their shared memory
-// fits, so that one block's loads overlap the other's transforms), at most 64 registers.
+// Blocks of PT = 1024 threads (one per SM), 512 (two per SM when their shared memory
+// fits, so that one block's loads overlap the other's transforms) or 256, at most 64
+// registers.
 template <typename T, typename TF, int PRO, int PT>
 __global__ void __launch_bounds__(PT, PLANE_MIN_BLOCKS(PT))
     zyfwd_cl_kernel(Grid<T> g, ClusterGeo cq, const SlotDev<TF> *__restrict__ tab,
