@@ -169,6 +169,36 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     const long long v0 = (long long)local * VEC_CHUNK;
     const long long v1 = min(V, v0 + VEC_CHUNK);
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    if constexpr (sizeof(T) == 4) {
+      // four consecutive points a thread, one 16-byte load per component plane and vector
+      // (each plane starts on a 16-byte boundary when V is a multiple of 4, and so does every
+      // item): four times the bytes in flight of one point a thread
+      if ((V & 3) == 0) {
+        for (long long v = v0 + 4 * threadIdx.x; v < v1; v += 4 * blockDim.x) {
+          float4 pt[6], r1[6], r2[6];
+#pragma unroll
+          for (int c = 0; c < 6; ++c) {
+            pt[c] = *reinterpret_cast<const float4 *>(kr.Y + c * V + v);
+            r1[c] = *reinterpret_cast<const float4 *>(kr.P + c * V + v);
+            r2[c] = *reinterpret_cast<const float4 *>(kr.Q + c * V + v);
+          }
+#pragma unroll
+          for (int c = 0; c < 6; ++c) {
+            const float4 y = make_float4(pt[c].x - c1 * r1[c].x, pt[c].y - c1 * r1[c].y,
+                                         pt[c].z - c1 * r1[c].z, pt[c].w - c1 * r1[c].w);
+            *reinterpret_cast<float4 *>(kr.Y + c * V + v) = y;
+            a0 += (double)r2[c].x * (double)y.x + (double)r2[c].y * (double)y.y +
+                  (double)r2[c].z * (double)y.z + (double)r2[c].w * (double)y.w;
+            a1 += (double)y.x * (double)y.x + (double)y.y * (double)y.y +
+                  (double)y.z * (double)y.z + (double)y.w * (double)y.w;
+            a2 += (double)r2[c].x * (double)r2[c].x + (double)r2[c].y * (double)r2[c].y +
+                  (double)r2[c].z * (double)r2[c].z + (double)r2[c].w * (double)r2[c].w;
+          }
+        }
+        finish_inverse<T, EPI_MINRES>(S, a0, a1, a2, local, per, red);
+        continue;
+      }
+    }
     for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
       T pt[6], r1[6], r2[6];
 #pragma unroll

@@ -276,14 +276,17 @@ template <typename T> static ClusterGeo cluster_geo(const GridPlan &p, int C) {
   return q;
 }
 
-// Threads of a cluster block: 512 when two blocks fit an SM's shared memory, else 1024
-// (SSFFT_CLUSTER_THREADS=256, 512 or 1024 overrides).
+// Threads of a cluster block: for float transforms 256 when three blocks fit an SM's
+// shared memory (128^3 on 4-block clusters: each radix-16 stage then has one butterfly per
+// thread, where 512 threads left half of them idle; measured 7-8% faster per pass), else
+// 512 when two fit, else 1024 (SSFFT_CLUSTER_THREADS=256, 512 or 1024 overrides).
 template <typename T> static int cluster_threads(const GridPlan &p, int C) {
   const int hs = (p.nz % 2 == 0) ? p.nz / 2 : p.hz;
-  const bool two = smem_cplane_bytes<T>(p.ny, p.nz, hs, C) <= 113 * 1024;
+  const size_t bytes = smem_cplane_bytes<T>(p.ny, p.nz, hs, C);
   const int want = env_int("SSFFT_CLUSTER_THREADS");
   if (want == 1024 || want == 512 || want == 256) return want;
-  return two ? 512 : 1024;
+  if (sizeof(T) == 4 && bytes <= 75 * 1024) return 256;
+  return bytes <= 113 * 1024 ? 512 : 1024;
 }
 
 // Threads of an x-pass block: 256, or 192 / 384 on float grids when SSFFT_XPASS_THREADS
@@ -884,7 +887,9 @@ static int launch_projector(const LaunchCtx &c, const SlotDev<TF> *tab, ExtIO<TF
                             cudaEvent_t *ev = nullptr) {
   const GridPlan &p = *c.p;
   const Grid<T> &g = grid_of<T>(p);
-  constexpr bool KRY = PRO_IS_KRYLOV(PRO);
+  // the middle passes of a Krylov matvec skip finished solves as the outer ones do (a
+  // device-side loop runs its chunk of iterations to the end after a solve finishes)
+  constexpr bool KRY = PRO_IS_KRYLOV(PRO) || PRO == PRO_TAU;
   auto rec = [&](int k) {
     if (ev) cudaEventRecord(ev[k], c.stream);
   };
