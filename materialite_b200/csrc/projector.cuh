@@ -564,7 +564,9 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
     const int k = udiv(item, g.fd_it_y);
     const int local = item - k * per;
     const SlotDev<TF> &S = tab[list.ids[k]];
-    if (KRY && slot_done(S.st)) continue;
+    // a finished solve's items are skipped: the flag is read here and tested after the tile
+    // copy, so the read's latency overlaps the copy (the flag does not change in a launch)
+    const int done = KRY ? __ldcg(&S.st->done) : 0;
     const int c = udiv(local, g.fd_nkynx);
     const int r1 = local - c * g.nky * g.nx;
     const int x = udiv(r1, g.fd_nky);
@@ -586,6 +588,7 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
       cp_async_wait_all();
     }
     __syncthreads();
+    if (done) continue;
     const LineLayout L(nk, nk, 0, 1, nk, g.fd_ky[ti], g.fd_ky[ti]);
     cplx<T> *res = smem_fft<T, INV, true>(bufA, bufB, L, g.py, tw);
     for (int e = threadIdx.x; e < ny * nk; e += blockDim.x) {
@@ -662,7 +665,9 @@ __global__ void __launch_bounds__(PT)
     const int kk_slot = udiv(item, g.fd_it_x);
     const int local = item - kk_slot * per;
     const SlotDev<TF> &S = tab[list.ids[kk_slot]];
-    if (KRY && slot_done(S.st)) continue;
+    // a finished solve's items are skipped: the flag is read here and tested after the tile
+    // copy, so the read's latency overlaps the copy (the flag does not change in a launch)
+    const int done = KRY ? __ldcg(&S.st->done) : 0;
     const int y = udiv(local, g.fd_nkx);
     const int kb = local - y * g.nkx;
     const int k0 = kb * g.kx;
@@ -686,6 +691,7 @@ __global__ void __launch_bounds__(PT)
       cp_async_wait_all();
     }
     __syncthreads();
+    if (done) continue;
     const LineLayout L(6 * nk, nk, sst, 1, nk, g.fd_x6k[ti], g.fd_kx[ti]);
     cplx<T> *res = smem_fft<T, false, true>(bufA, bufB, L, g.px, tw);
     cplx<T> *other = (res == bufA) ? bufB : bufA;
