@@ -16,6 +16,10 @@ implementation applies when ``x0=None``, ``M=None``, ``shift=0``, ``check=False`
 ``||A||`` is the running Frobenius estimate of the Lanczos tridiagonal matrix and
 ``cond(A)`` the ratio of the largest to smallest rotation pivot.  ``tests/test_oracle.py``
 checks this function against scipy on random symmetric systems.
+
+``atol`` > 0 (not part of the reference) adds the absolute floor that the product's served
+requests put on the same tests: stop 1 also when ||r|| <= atol, and no iteration at all when
+beta1 <= atol.
 """
 
 import math
@@ -23,7 +27,7 @@ import math
 import numpy as np
 
 
-def minres(matvec, b, rtol, maxiter=None):
+def minres(matvec, b, rtol, maxiter=None, atol=0.0):
     """Solve ``A x = b`` for symmetric ``A`` given as ``matvec``; returns ``(x, iterations)``."""
     b = np.asarray(b, dtype=np.float64)
     n = b.size
@@ -35,6 +39,8 @@ def minres(matvec, b, rtol, maxiter=None):
     if beta1_sq == 0.0:
         return x, 0
     beta1 = math.sqrt(beta1_sq)
+    if beta1 <= atol:
+        return x, 0
 
     # Lanczos state: r_prev / r_cur are the unnormalised previous / current vectors.
     r_prev = b
@@ -111,6 +117,8 @@ def minres(matvec, b, rtol, maxiter=None):
             if test2 <= rtol:
                 stop = 2
             if test1 <= rtol:
+                stop = 1
+            if rnorm <= atol:
                 stop = 1
         if stop != 0:
             break
