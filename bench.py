@@ -454,7 +454,8 @@ def serve_mode(args, w):
 
     import torch
     srv = RVEServer(device=local, max_slots=w["slots"], precision="mixed",
-                    krylov_floor=args.krylov_floor)
+                    krylov_floor=args.krylov_floor,
+                    krylov_forcing=args.krylov_forcing)
     warm = list(classes.values())
     for _ in range(args.warmup):
         one_pass(srv, warm, False, saturate=True)
@@ -496,7 +497,7 @@ def serve_mode(args, w):
     sub = reqs[:min(len(reqs), w["plain_count"])]
     comps_sub, span_sub = one_pass(srv, sub, True, saturate=True)
     stress_mixed = [r.stress.copy() for r in sub]
-    krylov_floor = srv.krylov_floor
+    krylov_floor, krylov_forcing = srv.krylov_floor, srv.krylov_forcing
     srv.close()
     secs_plain, pouts = solve_plain(sub, "fp64", device=local)
     stress_fp64 = [r.stress.copy() for r in sub]
@@ -509,7 +510,8 @@ def serve_mode(args, w):
     cpu_gpu = None
     if cpu_reqs:
         srv2 = RVEServer(device=local, max_slots=w["slots"], precision="mixed",
-                         krylov_floor=args.krylov_floor)
+                         krylov_floor=args.krylov_floor,
+                         krylov_forcing=args.krylov_forcing)
         _, span_c = one_pass(srv2, cpu_reqs, False, saturate=True)
         srv2.close()
         secs_c, _ = solve_plain(cpu_reqs, "fp64", device=local, keep_stress=False)
@@ -532,6 +534,7 @@ def serve_mode(args, w):
                                     "strain/stress fields, residuals, norms, Krylov scalars "
                                     "and crystal-plasticity Newton",
                        "krylov_floor": krylov_floor,
+                       "krylov_forcing": krylov_forcing,
                        "l2": "inputs larger than L2: the stream's fields stream through HBM"},
             "served": {"solves_per_s": value, **lat, "makespan_s": t_max,
                        "per_class_latency": per_class},
@@ -585,7 +588,8 @@ def sweep_mode(args, w):
     count = args.count or 64
     rates = [float(x) for x in args.rates.split(",")]
     srv = RVEServer(device=0, max_slots=w["slots"], precision="mixed",
-                    krylov_floor=args.krylov_floor)
+                    krylov_floor=args.krylov_floor,
+                    krylov_forcing=args.krylov_forcing)
     run_stream(srv, request_stream(min(count, 8), 0.0, seed=w["seed"]), timeout=1800)
     out = {"workload": f"serve sweep: {count} requests of the serving stream, "
                        f"{w['slots']} slots per class, mixed precision", "rates": []}
@@ -628,7 +632,8 @@ def classes_mode(args, w):
         secs, pouts = secs[1:], pouts[1:]
         ref = [r.stress.copy() for r in rs]
         srv = RVEServer(device=0, max_slots=w["slots"], precision="mixed",
-                        krylov_floor=args.krylov_floor)
+                        krylov_floor=args.krylov_floor,
+                        krylov_forcing=args.krylov_forcing)
         run_stream(srv, warm, timeout=3600)
         for r in rs:
             r.keep_stress = True
@@ -664,7 +669,8 @@ def group_mode(args, w):
         t += 1
     reqs = request_stream(len(tags), w["rate"], seed=w["seed"], workers=host_workers(), tags=tags)
     srv = RVEServer(device=0, max_slots=w["slots"], precision=args.precision,
-                    krylov_floor=args.krylov_floor)
+                    krylov_floor=args.krylov_floor,
+                    krylov_forcing=args.krylov_forcing)
     for r in reqs:
         r.arrival = 0.0
     comps, span = run_stream(srv, reqs, timeout=3600)
@@ -816,6 +822,8 @@ def main():
     ap.add_argument("--tag", type=int, default=0, help="request mode: index in the stream")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--kind", default="evp64", help="group mode: request class (e.g. evp64)")
+    ap.add_argument("--krylov-forcing", type=float, default=None,
+                    help="served requests' MINRES relative forcing; default: the server's")
     ap.add_argument("--krylov-floor", type=float, default=None,
                     help="served requests' MINRES floor (fraction of the tolerance); "
                          "default: the server's (0.1 mixed, 0 FP64)")

@@ -85,6 +85,10 @@ typedef struct {
    * keeps the next equilibrium error at or below krylov_floor * global_tolerance.  0 (the
    * reference's test alone, small_strain_fft.py:289-293) unless set. */
   double krylov_floor;
+  /* Relative forcing of the MINRES stopping test (inexact Newton): a solve also stops once
+   * |b - A x|_2 <= krylov_forcing * |b|_2.  0 (the reference's test alone) unless set; in
+   * [0, 1). */
+  double krylov_forcing;
 } ssfft_config;
 
 /* Per load step inputs: the LoadSchedule closures evaluated at (t, dt)

@@ -59,6 +59,7 @@ class SsfftConfig(ctypes.Structure):
         ("linear_solver_tolerance", ctypes.c_double),
         ("stress_mask", ctypes.c_double * 6),
         ("krylov_floor", ctypes.c_double),
+        ("krylov_forcing", ctypes.c_double),
     ]
 
 

@@ -608,12 +608,14 @@ struct Group {
       b.md.rtol = cfg.linear_solver_tolerance;
       b.md.maxiter = maxiter;
       b.md.atol_scale = krylov_atol_scale(cfg);
+      b.md.forcing = cfg.krylov_forcing;
       CK(cudaMemcpyAsync((char *)dtab + s * desc_bytes(), &b.md, sizeof(b.md),
                          cudaMemcpyHostToDevice, stream));
     } else {
       b.mf.rtol = std::max(cfg.linear_solver_tolerance, MIXED_RTOL_FLOOR);
       b.mf.maxiter = maxiter;
       b.mf.atol_scale = krylov_atol_scale(cfg);
+      b.mf.forcing = cfg.krylov_forcing;
       CK(cudaMemcpyAsync((char *)dtab + s * desc_bytes(), &b.mf, sizeof(b.mf),
                          cudaMemcpyHostToDevice, stream));
     }

@@ -100,8 +100,9 @@ __global__ void __launch_bounds__(SSFFT_THREADS)
         s.itn = 0;
         s.maxiter = S.maxiter;
         s.istop = 0;
-        // absolute floor: the stress scale of the residual just computed
+        // absolute floor (the stress scale of the residual just computed) and relative forcing
         s.atol = S.atol_scale > 0.0 ? S.atol_scale * mean_von_mises(S.results, V) : 0.0;
+        s.atol = fmax(s.atol, S.forcing * beta1);
         // beta1 == 0: x = 0 is exact; beta1 under the floor: x = 0 is close enough
         s.done = (b2 == 0.0 || beta1 <= s.atol) ? 1 : 0;
         if (s.done && b2 != 0.0) s.istop = 1;

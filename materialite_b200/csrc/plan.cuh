@@ -340,6 +340,8 @@ static int validate_config(const ssfft_config *cfg) {
       return ssfft_internal_fail(SSFFT_E_INVALID, "stress mask can only have zeros and ones");
   if (!(cfg->krylov_floor >= 0.0 && cfg->krylov_floor < 1.0))
     return ssfft_internal_fail(SSFFT_E_INVALID, "krylov_floor must be in [0, 1)");
+  if (!(cfg->krylov_forcing >= 0.0 && cfg->krylov_forcing < 1.0))
+    return ssfft_internal_fail(SSFFT_E_INVALID, "krylov_forcing must be in [0, 1)");
   AxisPlan p;
   for (int d = 0; d < 3; ++d)
     if (!make_axis_plan(cfg->n[d], p))

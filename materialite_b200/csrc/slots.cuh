@@ -71,6 +71,7 @@ template <typename T> struct SlotDev {
   long long maxiter;
   double atol_scale;            // MINRES also stops once |r| <= atol_scale x mean von Mises
                                 // stress (0: off)
+  double forcing;               // ... or once |r| <= forcing x |b| (0: off)
 };
 
 // The slots a launch works on: ids[0 .. *count).  Both live in device memory, so a kernel

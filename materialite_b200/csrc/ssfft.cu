@@ -326,6 +326,7 @@ template <typename T> static int step_impl(ssfft_handle *h, const ssfft_step_in 
   m.rtol = h->plan.fp64 ? h->cfg.linear_solver_tolerance
                         : std::max(h->cfg.linear_solver_tolerance, MIXED_RTOL_FLOOR);
   m.atol_scale = krylov_atol_scale(h->cfg);
+  m.forcing = h->cfg.krylov_forcing;
   CKR(upload(h));
   CKR(launch_strain_guess<T>(c, dtab<T>(h)));
 
@@ -927,6 +928,7 @@ template <typename T> static int profile_impl(ssfft_handle *h, int reps, double 
   for (int k = 0; k < 6; ++k) m.sbar[k] = 0.0;
   m.rtol = 0.0;
   m.atol_scale = 0.0;
+  m.forcing = 0.0;
   m.maxiter = (long long)1 << 60;
   CKR(upload(h));
   CKR(launch_residual<T>(c, dtab<T>(h)));

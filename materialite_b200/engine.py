@@ -65,9 +65,10 @@ class SolverHandle:
     def __init__(self, dims, stress_mask, precision="mixed", global_tolerance=1.0e-3,
                  strain_correction_tolerance=1.0e-2, linear_solver_tolerance=1.0e-5,
                  max_newton_iterations=100, max_krylov_iterations=0, device=0,
-                 krylov_floor=0.0):
-        """``krylov_floor`` > 0 adds an absolute floor to the MINRES stopping test
-        (ssfft_config.krylov_floor); 0 keeps the reference's test alone."""
+                 krylov_floor=0.0, krylov_forcing=0.0):
+        """``krylov_floor`` > 0 adds an absolute floor and ``krylov_forcing`` > 0 a relative
+        forcing term to the MINRES stopping test (ssfft_config.krylov_floor,
+        .krylov_forcing); 0 keeps the reference's test alone."""
         self.lib = nat.load_library()
         cfg = nat.SsfftConfig()
         for d in range(3):
@@ -80,6 +81,7 @@ class SolverHandle:
         cfg.strain_correction_tolerance = float(strain_correction_tolerance)
         cfg.linear_solver_tolerance = float(linear_solver_tolerance)
         cfg.krylov_floor = float(krylov_floor)
+        cfg.krylov_forcing = float(krylov_forcing)
         for c in range(6):
             cfg.stress_mask[c] = float(stress_mask[c])
         self.cfg = cfg
@@ -153,7 +155,7 @@ class SolverHandle:
 
     def set_options(self, stress_mask=None, global_tolerance=None,
                     strain_correction_tolerance=None, linear_solver_tolerance=None,
-                    krylov_floor=None):
+                    krylov_floor=None, krylov_forcing=None):
         """Change the stress mask and tolerances of the handle (same grid and precision)."""
         cfg = self.cfg
         if stress_mask is not None:
@@ -167,6 +169,8 @@ class SolverHandle:
             cfg.linear_solver_tolerance = float(linear_solver_tolerance)
         if krylov_floor is not None:
             cfg.krylov_floor = float(krylov_floor)
+        if krylov_forcing is not None:
+            cfg.krylov_forcing = float(krylov_forcing)
         nat.check(self.lib.ssfft_set_options(self.h, ctypes.byref(cfg)))
 
     def solve_constant_rates(self, strain_rate, stress_rate, end_time, initial_time_increment,

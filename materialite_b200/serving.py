@@ -25,6 +25,10 @@ from .microstructure import periodic_voronoi, quaternion_random_rotations
 # test spends 30-45 iterations resolving that round-off.
 SERVED_KRYLOV_FLOOR = 0.1
 
+# Relative forcing of served mixed-precision requests' linear solves (inexact Newton): a
+# solve also stops once its residual is this fraction of its right-hand side.  0: off.
+SERVED_KRYLOV_FORCING = 0.0
+
 
 class SsfftPhase(ctypes.Structure):
     _fields_ = [
@@ -129,10 +133,11 @@ def _phase_struct(p):
 
 class RVEServer:
     def __init__(self, device=0, max_slots=16, hbm_budget_bytes=0, precision="mixed",
-                 krylov_floor=None):
-        """``krylov_floor``: the MINRES absolute floor of every request
-        (ssfft_config.krylov_floor); None gives SERVED_KRYLOV_FLOOR in mixed precision and 0
-        (the reference's stopping test alone) in FP64."""
+                 krylov_floor=None, krylov_forcing=None):
+        """``krylov_floor`` / ``krylov_forcing``: the MINRES absolute floor and relative
+        forcing of every request (ssfft_config.krylov_floor, .krylov_forcing); None gives
+        SERVED_KRYLOV_FLOOR / SERVED_KRYLOV_FORCING in mixed precision and 0 (the reference's
+        stopping test alone) in FP64."""
         self.lib = _bind(nat.load_library())
         h = ctypes.c_void_p()
         nat.check(self.lib.ssfft_server_create(int(device), int(max_slots),
@@ -142,6 +147,9 @@ class RVEServer:
         if krylov_floor is None:
             krylov_floor = SERVED_KRYLOV_FLOOR if precision != "fp64" else 0.0
         self.krylov_floor = float(krylov_floor)
+        if krylov_forcing is None:
+            krylov_forcing = SERVED_KRYLOV_FORCING if precision != "fp64" else 0.0
+        self.krylov_forcing = float(krylov_forcing)
         self._keep = {}
 
     def clock(self):
@@ -158,6 +166,7 @@ class RVEServer:
         cfg.strain_correction_tolerance = 1e-2
         cfg.linear_solver_tolerance = r.linear_solver_tolerance
         cfg.krylov_floor = self.krylov_floor
+        cfg.krylov_forcing = self.krylov_forcing
         for c in range(6):
             cfg.stress_mask[c] = float(r.stress_mask[c])
         req.n_phases = len(r.phases)

@@ -508,13 +508,14 @@ def solve(dims, R, model, load, end_time=1.0, initial_time_increment=None,
           max_time_increment=None, min_time_increment=1.0e-9, start_time=0.0,
           global_tolerance=1.0e-3, strain_correction_tolerance=1.0e-2,
           linear_solver_tolerance=1.0e-5, output_times=None, output_variables=None,
-          stats=None, krylov_maxiter=None, krylov_floor=0.0):
+          stats=None, krylov_maxiter=None, krylov_floor=0.0, krylov_forcing=0.0):
     """Oracle of ``SmallStrainFFT.run`` (small_strain_fft.py:60-264).  ``model`` is an
     Elastic/EVP/Multiphase oracle; returns a dict of final fields, or of per-output-time
     stacks when ``output_times`` is given.  ``krylov_floor`` > 0 (not part of the reference)
     adds the product's served-request floor to each MINRES solve: an absolute residual
     tolerance of krylov_floor * global_tolerance * the mean von Mises stress of the stress
-    the right-hand side was computed from."""
+    the right-hand side was computed from; ``krylov_forcing`` > 0 its relative forcing, a
+    residual tolerance of krylov_forcing * |b|."""
     dims = tuple(int(d) for d in dims)
     V = int(np.prod(dims))
     dt = end_time if initial_time_increment is None else initial_time_increment
@@ -578,6 +579,9 @@ def solve(dims, R, model, load, end_time=1.0, initial_time_increment=None,
             if krylov_floor > 0.0:
                 atol = krylov_floor * global_tolerance * \
                     dev_norm(stress.mean(axis=0)) * math.sqrt(1.5)
+            if krylov_forcing > 0.0:
+                bf = np.ravel(b)
+                atol = max(atol, krylov_forcing * math.sqrt(float(bf @ bf)))
             x, kits = minres(matvec, b, linear_solver_tolerance, krylov_maxiter, atol=atol)
             if stats is not None:
                 stats["krylov"].append(kits)

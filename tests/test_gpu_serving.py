@@ -191,3 +191,26 @@ def test_krylov_floor_keeps_the_fp64_result():
         assert err <= 1e-6, (r.tag, err)
         assert c.result.krylov_iterations < po.krylov_iterations
     assert comps[0].result.newton_iterations == pouts[0].newton_iterations  # elastic
+
+
+def test_krylov_forcing_stays_within_tolerance():
+    """The relative forcing (inexact Newton: each linear solve also ends once its residual is
+    1% of its right-hand side) on top of the floor: the same increments and cutbacks as the
+    plain FP64 solve, stresses within 2e-6 of it, and fewer Krylov iterations than the floor
+    alone for the crystal-plasticity request."""
+    plain = small_requests()[:2]
+    _, pouts = solve_plain(plain, precision="fp64")
+    runs = []
+    for forcing in (0.0, 0.01):
+        reqs = small_requests()[:2]
+        server = RVEServer(max_slots=2, krylov_forcing=forcing)
+        comps, _ = run_stream(server, reqs)
+        server.close()
+        runs.append((reqs, sorted(comps, key=lambda c: c.tag)))
+    reqs, comps = runs[1]
+    for r, p, c, po in zip(reqs, plain, comps, pouts):
+        assert c.status == 0
+        assert c.result.steps == po.steps and c.result.cutbacks == po.cutbacks
+        err = np.linalg.norm(r.stress - p.stress) / np.linalg.norm(p.stress)
+        assert err <= 2e-6, (r.tag, err)
+    assert comps[1].result.krylov_iterations < runs[0][1][1].result.krylov_iterations

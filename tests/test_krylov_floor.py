@@ -1,8 +1,9 @@
-"""The served requests' MINRES floor, checked on the CPU through the oracle: against the
-reference-written golden fields of configs 1 and 3, a solve whose linear solves also stop at
-the floor (residual <= 0.1 x tolerance x mean von Mises stress) takes the same Newton
-iterations and fewer Krylov iterations, and its stress stays within 1e-7 of the
-reference's.  The GPU side of the same claim is test_gpu_serving.py's floor test."""
+"""The served requests' MINRES floor and relative forcing, checked on the CPU through the
+oracle: against the reference-written golden fields of configs 1 and 3, a solve whose linear
+solves also stop at the floor (residual <= 0.1 x tolerance x mean von Mises stress) takes the
+same Newton iterations and fewer Krylov iterations, and its stress stays within 1e-7 of the
+reference's; with a relative forcing of 0.01 on top (residual <= 0.01 |b|) fewer still,
+within 1e-6.  The GPU side of the same claims is in test_gpu_serving.py."""
 
 import pytest
 
@@ -12,7 +13,7 @@ from test_oracle import config3_model, golden, per_point_rotations, rel
 FLOOR = 0.1  # materialite_b200.serving.SERVED_KRYLOV_FLOOR
 
 
-def run(case, floor):
+def run(case, floor, forcing=0.0):
     stats = {}
     if case == "elastic":
         g = golden("config1_elastic16")
@@ -20,13 +21,13 @@ def run(case, floor):
                       O.ElasticOracle(O.cubic_stiffness(250.0, 150.0, 120.0)),
                       O.LoadOracle.uniaxial(1e-3, "x"), end_time=10.0,
                       initial_time_increment=1.0, global_tolerance=1e-6, stats=stats,
-                      krylov_floor=floor)
+                      krylov_floor=floor, krylov_forcing=forcing)
     else:
         g = golden("config3_evp8")
         out = O.solve((8, 8, 8), per_point_rotations(g), config3_model(),
                       O.LoadOracle.uniaxial(1e-3, "x"), end_time=4.0,
                       initial_time_increment=0.2, global_tolerance=1e-6, stats=stats,
-                      krylov_floor=floor)
+                      krylov_floor=floor, krylov_forcing=forcing)
     return out, stats, g
 
 
@@ -43,6 +44,16 @@ def test_floor_keeps_the_reference_result(case):
         # right-hand side is under the floor
         assert sum(st1["krylov"]) * 10 < sum(st0["krylov"])
         assert all(k == 0 for k in st1["krylov"][3:])
+
+
+def test_forcing_keeps_the_reference_result():
+    """Inexact Newton on config 3: the relative forcing ends each linear solve at 1% of its
+    right-hand side; the Newton iterations stay within 5% and the stress within 1e-6."""
+    out0, st0, g = run("evp", FLOOR)
+    out1, st1, _ = run("evp", FLOOR, 0.01)
+    assert rel(out1["stress"], g["stress"]) < 1e-6
+    assert sum(st1["newton"]) <= 1.05 * sum(st0["newton"])
+    assert sum(st1["krylov"]) < 0.8 * sum(st0["krylov"])
 
 
 def test_floor_on_the_minres_restatement():

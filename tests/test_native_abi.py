@@ -67,13 +67,14 @@ def test_config_validation(n, mask, code):
     assert nat.load_library().ssfft_last_error()
 
 
-@pytest.mark.parametrize("floor", [-0.1, 1.0, float("nan")])
-def test_krylov_floor_validation(floor):
+@pytest.mark.parametrize("field", ["krylov_floor", "krylov_forcing"])
+@pytest.mark.parametrize("value", [-0.1, 1.0, float("nan")])
+def test_krylov_stop_option_validation(field, value):
     cfg = config()
-    cfg.krylov_floor = floor
+    setattr(cfg, field, value)
     rc, _ = estimate(cfg)
     assert rc == -1
-    assert b"krylov_floor" in nat.load_library().ssfft_last_error()
+    assert field.encode() in nat.load_library().ssfft_last_error()
 
 
 def test_invalid_precision_rejected():
