@@ -6,8 +6,9 @@ import numpy as np
 import pytest
 
 from materialite_b200.engine import SolverHandle, solve, unique_rotations
-from materialite_b200.serving import (SERVED_KRYLOV_FLOOR, RVEServer, elastic_phase,
-                                      evp_phase, make_request, run_stream, solve_plain)
+from materialite_b200.serving import (SERVED_KRYLOV_FLOOR, SERVED_KRYLOV_FORCING, RVEServer,
+                                      elastic_phase, evp_phase, make_request, run_stream,
+                                      solve_plain)
 
 pytestmark = pytest.mark.gpu
 
@@ -52,7 +53,7 @@ def test_native_time_loop_matches_python_loop():
     assert comps[0].status == 0
     h = SolverHandle(r.dims, r.stress_mask, "mixed", global_tolerance=r.global_tolerance,
                      linear_solver_tolerance=r.linear_solver_tolerance,
-                     krylov_floor=SERVED_KRYLOV_FLOOR)
+                     krylov_floor=SERVED_KRYLOV_FLOOR, krylov_forcing=SERVED_KRYLOV_FORCING)
     h.set_phases(r.phases)
     table, idx = unique_rotations(r.rotations[r.grain])
     h.set_microstructure(table, idx)
@@ -134,7 +135,7 @@ def test_group_time_loop_matches_python_loop_crystal_plasticity():
     assert comps[0].status == 0
     h = SolverHandle(r.dims, r.stress_mask, "mixed", global_tolerance=r.global_tolerance,
                      linear_solver_tolerance=r.linear_solver_tolerance,
-                     krylov_floor=SERVED_KRYLOV_FLOOR)
+                     krylov_floor=SERVED_KRYLOV_FLOOR, krylov_forcing=SERVED_KRYLOV_FORCING)
     h.set_phases(r.phases)
     table, idx = unique_rotations(r.rotations[r.grain])
     h.set_microstructure(table, idx)
@@ -180,7 +181,7 @@ def test_krylov_floor_keeps_the_fp64_result():
     reqs = small_requests()[:2]  # one elastic, one crystal-plasticity request
     plain = small_requests()[:2]
     _, pouts = solve_plain(plain, precision="fp64")
-    server = RVEServer(max_slots=2)
+    server = RVEServer(max_slots=2, krylov_forcing=0.0)  # the floor alone
     comps, _ = run_stream(server, reqs)
     server.close()
     comps = sorted(comps, key=lambda c: c.tag)
