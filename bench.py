@@ -563,7 +563,8 @@ def serve_mode(args, w):
             "served_over_plain": served_sub / plain_value,
             # the stream's steady served rate over the plain rate of the same prefix's mix
             "served_stream_over_plain": value / plain_value,
-            "stress_rel_l2_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs)),
+            "stress_rel_l2_mixed_vs_fp64": {"max": max(errs) if errs else None,
+                                            "median": float(np.median(errs)) if errs else None,
                                             "requests": len(errs)},
             "cpu_class_on_gpu": cpu_gpu,
             "failed_requests": {"count": len(failures),
