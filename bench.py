@@ -3,7 +3,7 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload serve|plain128|...] [--mode bench|kernels|request|accuracy|sweep]
 
-Default workload: the serving stream of BASELINE config 4 -- 512 RVE requests arriving as
+Default workload: the RVE serving stream -- 512 homogenisation requests arriving as
 a Poisson process at 50 req/s, N ~ U{32,48,64,96}, 20-400 periodic Voronoi grains,
 elastic or FCC crystal plasticity, uniaxial or biaxial strain rate, 10-50 load steps --
 served on one warm server.  The K timed steps are K consecutive slices of that stream (by
@@ -351,8 +351,8 @@ def reference_arm_single(args, w):
 
 
 def serve_config(w, count):
-    return {"workload": f"serve: {count} requests of the seeded serving stream (BASELINE config "
-                        f"4), Poisson arrivals at {w['rate']} req/s, N in {{32,48,64,96}}, 20-400 "
+    return {"workload": f"serve: {count} requests of the seeded RVE serving stream, Poisson "
+                        f"arrivals at {w['rate']} req/s, N in {{32,48,64,96}}, 20-400 "
                         "periodic Voronoi grains, elastic or FCC EVP, uniaxial/biaxial strain "
                         "rate 1e-3, 10-50 load steps; one step = one slice of the stream by "
                         "arrival, the stream run once continuously",
@@ -407,7 +407,7 @@ def reference_arm(args, w):
 
 
 def serve_mode(args, w):
-    """Serving benchmark of BASELINE config 4 on one warm server (mixed precision): the
+    """Serving benchmark of the RVE request stream on one warm server (mixed precision): the
     W warm-up steps serve one request of every class of the stream at once; the K timed
     steps are the whole stream at its Poisson arrivals (one continuous run).  Then: the same
     stream's prefix end to end with every stress field read back, the sweep of arrival

@@ -1,5 +1,6 @@
 """The served requests' MINRES floor and relative forcing, checked on the CPU through the
-oracle: against the reference-written golden fields of configs 1 and 3, a solve whose linear
+oracle: against the reference-written golden fields of the 16^3 cubic-elastic case (10
+increments) and the 8^3 FCC crystal-plasticity case (20 increments), a solve whose linear
 solves also stop at the floor (residual <= 0.1 x tolerance x mean von Mises stress) takes the
 same Newton iterations and fewer Krylov iterations, and its stress stays within 1e-7 of the
 reference's; with a relative forcing of 0.01 on top (residual <= 0.01 |b|) fewer still,
@@ -47,8 +48,9 @@ def test_floor_keeps_the_reference_result(case):
 
 
 def test_forcing_keeps_the_reference_result():
-    """Inexact Newton on config 3: the relative forcing ends each linear solve at 1% of its
-    right-hand side; the Newton iterations stay within 5% and the stress within 1e-6."""
+    """Inexact Newton on the 8^3 crystal-plasticity case: the relative forcing ends each
+    linear solve at 1% of its right-hand side; the Newton iterations stay within 5% and the
+    stress within 1e-6."""
     out0, st0, g = run("evp", FLOOR)
     out1, st1, _ = run("evp", FLOOR, 0.01)
     assert rel(out1["stress"], g["stress"]) < 1e-6
